@@ -1,0 +1,379 @@
+"""Benchmark: Mrays/s of the plain GPU path on the mid scene (1920x1080, 64 spp,
+GI on, 4 bounces), with the oracle's CPU time of the same workload beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config mid|small]
+
+A step is one full frame: every pass of every pixel, accumulated and encoded
+to RGBA8 on the device. Rays are BVH queries: camera and bounce rays
+(closest hit) plus shadow rays (any hit). `value` is device time (CUDA events
+on the library's stream around each frame) with the scene resident in HBM and
+the image left on the device; `e2e` is the public `raytrace_compiled` call
+with the image read back to host memory. L2 is flushed between steps.
+
+Multi-GPU: every rank renders its own frame (replicas; the path has no data
+exchange), value = all ranks' rays / the slowest rank's time.
+`--impl reference` times the reference's algorithm on the host cores: the
+reference is TypeScript and no Node.js is installed, so this is the oracle
+(a C++ restatement of it) on all host threads, on a bounded sample of pixels.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from typing import Any, Dict, List, Optional, Tuple
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mrays/s (closest-hit + shadow BVH queries per second)"
+UNIT = "Mrays/s"
+# Algorithmic bytes per BVH query (per node visit: one 32-byte box + reference
+# word; per triangle test: 36 bytes of v0, e1, e2), with the visit counts of
+# the reference algorithm measured by the oracle on a sample of the same rays.
+BOX_BYTES = 32
+TRI_BYTES = 36
+
+
+def dist_env() -> Tuple[int, int, int]:
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peaks() -> Dict[str, Any]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def load_config(name: str):
+    from meercadraytracer_b200 import scenes
+
+    if name == "small":
+        return scenes.small_scene()
+    if name == "mid":
+        return scenes.mid_scene()
+    raise SystemExit(f"unknown config {name}")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc: Optional[subprocess.Popen] = None
+        self.lines: List[str] = []
+        self._t: Optional[threading.Thread] = None
+
+    def start(self) -> None:
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self) -> None:
+        assert self.proc and self.proc.stdout
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> Dict[str, Any]:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def oracle_sample(compiled, camera, bench, seconds: float, threads: int, seed: int = 1
+                  ) -> Dict[str, Any]:
+    """Times the oracle on a random pixel subset of the workload (all passes), growing the
+    subset until the run takes about `seconds`. Returns rays/s and per-query visit counts."""
+    from meercadraytracer_b200.raytrace import as_options, output_srgb, sample_count, trace_settings
+    from oracle import cpu
+
+    o = as_options(bench.options)
+    st, spp, srgb = trace_settings(o), sample_count(o), output_srgb(o)
+    rng = np.random.default_rng(seed)
+    total = bench.width * bench.height
+    n = 64
+    while True:
+        idx = rng.choice(total, min(n, total), replace=False)
+        px, py = (idx % bench.width).astype(np.int32), (idx // bench.width).astype(np.int32)
+        ctr = cpu.oracle_counters()
+        t0 = time.perf_counter()
+        cpu.render_pixels(compiled, camera, st, bench.width, bench.height, spp, srgb, px, py, threads, ctr)
+        dt = time.perf_counter() - t0
+        if dt >= seconds * 0.5 or n >= total:
+            c = ctr.as_dict()
+            rays = c["closest_queries"] + c["any_queries"]
+            return {"seconds": dt, "pixels": int(idx.size), "samples": int(idx.size) * spp, "rays": rays,
+                    "mrays_s": rays / dt / 1e6, "counters": c, "threads": threads}
+        n = int(min(total, n * max(2.0, seconds / max(dt, 1e-3) * 0.8)))
+
+
+def bytes_per_query(counters: Dict[str, int]) -> Dict[str, float]:
+    cq, aq = max(1, counters["closest_queries"]), max(1, counters["any_queries"])
+    return {"closest": (BOX_BYTES * counters["closest_boxes"] + TRI_BYTES * counters["closest_tris"]) / cq,
+            "any": (BOX_BYTES * counters["any_boxes"] + TRI_BYTES * counters["any_tris"]) / aq}
+
+
+def run_reference(args, rank: int) -> None:
+    if rank != 0:
+        return
+    from meercadraytracer_b200.compile import compile_camera, compile_scene
+    from oracle import cpu
+
+    bench = load_config(args.config)
+    compiled = compile_scene(bench.scene, builder=cpu.compile_sink)
+    cam = compile_camera(bench.camera)
+    threads = os.cpu_count() or 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = oracle_sample(compiled, cam, bench, args.ref_seconds, threads, seed=100 + i)
+        if i >= args.warmup:
+            vals.append(r)
+    value = statistics.mean(v["mrays_s"] for v in vals)
+    sample = (f"{vals[0]['pixels']} random pixels x all {bench.options['samples']} passes per step "
+              f"({vals[0]['rays']} rays, {vals[0]['seconds']:.1f} s), oracle C++ restatement of the reference "
+              f"(TypeScript; no Node.js on the box)")
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * statistics.mean(v["seconds"] for v in vals), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded scene)", "config": {"workload": bench.name},
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int, local: int) -> None:
+    import ctypes as C
+
+    import torch
+
+    from meercadraytracer_b200 import abi
+    from meercadraytracer_b200.compile import compile_camera, compile_shading, flatten_meshes
+    from meercadraytracer_b200.executors import GpuExecutor
+    from meercadraytracer_b200.raytrace import as_options, output_srgb, raytrace_compiled, sample_count, trace_settings
+    from meercadraytracer_b200.types import CompiledScene
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+
+    bench = load_config(args.config)
+    o = as_options(bench.options)
+    st, spp, srgb = trace_settings(o), sample_count(o), output_srgb(o)
+    ex = GpuExecutor(local)
+    if args.capacity:
+        ex.set_capacity(args.capacity)
+    t0 = time.perf_counter()
+    shading, meshes = compile_shading(bench.scene)
+    ids = {id(m): i for i, m in enumerate(shading.material_objects)}
+    sink = flatten_meshes(meshes, lambda m: ids.get(id(m), 0))
+    t_flat = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    geometry = ex.compile_sink(sink)
+    t_build = time.perf_counter() - t0
+    compiled = CompiledScene(geometry, shading.materials, shading.textures, shading.environments, shading.lights,
+                             shading.background, shading.environment, shading.fog)
+    cam = compile_camera(bench.camera)
+    t0 = time.perf_counter()
+    ex.load_scene(compiled)
+    t_upload = time.perf_counter() - t0
+    w, h = bench.width, bench.height
+    image = torch.empty(w * h * 4, dtype=torch.uint8, device=f"cuda:{local}")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def frame() -> None:
+        ex.raytrace_device(compiled, cam, w, h, st, spp, srgb, image.data_ptr())
+
+    for _ in range(args.warmup):
+        frame()
+    # Timed region: K frames, device time from the library's CUDA events.
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ex.reset_stats()
+    clocks = ClockSampler(local)
+    clocks.start()
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        frame()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    s = ex.stats()
+    device_ms = s["ms_total"]
+    rays = s["closest_rays"] + s["any_rays"]
+    t = torch.tensor([device_ms, float(rays)], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t.clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        device_ms, all_rays = float(tmax[0]), float(tsum[1])
+    else:
+        all_rays = float(rays)
+    value = all_rays / (device_ms / 1000.0) / 1e6
+    launches = int(s["launches"])
+
+    # End to end through the public API: host image read back every step.
+    ex.reset_stats()
+    e2e_times = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        res = raytrace_compiled(compiled, cam, w, h, o, executor=ex)
+        e2e_times.append(time.perf_counter() - t1)
+    e2e_rays = ex.stats()
+    e2e_value = (e2e_rays["closest_rays"] + e2e_rays["any_rays"]) / sum(e2e_times) / 1e6 * world
+    h2d = C.sizeof(abi.mcrt_camera) + C.sizeof(abi.mcrt_settings)
+    d2h = int(res.data.nbytes)
+
+    # Kernel breakdown of one frame (events around every kernel) for the roofline.
+    ex.reset_stats()
+    ex.set_timing(True)
+    frame()
+    ex.set_timing(False)
+    k = ex.stats()
+    kernels = {name: {"ms": k[f"ms_{name}"], "launches": k[f"n_{name}"]}
+               for name in ("raygen", "extend", "shade", "shadow", "resolve", "accumulate")}
+    top = max(("extend", "shadow"), key=lambda n: kernels[n]["ms"])
+
+    if dist:
+        dist.barrier()
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        ex.dispose()
+        return
+
+    line: Dict[str, Any] = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(device_ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded scene, no dataset)",
+        "config": {"workload": bench.name, "triangles": bench.triangles, "width": w, "height": h, "spp": spp,
+                   "rays_per_step": rays / args.steps, "l2": "flushed between steps (512 MiB write)",
+                   "parallelism": "replicas" if world > 1 else "single GPU", "path_capacity": ex.stats()["path_bytes"],
+                   "compile_s": {"flatten_host": round(t_flat, 3), "gpu_bvh_compile": round(t_build, 3),
+                                 "upload": round(t_upload, 3)}},
+        "wall_s_timed": round(wall, 3),
+        "gpu_launches": launches,
+        "clocks": clk,
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "note": "scene resident in HBM (uploaded once per geometry/shading version, as the executor "
+                        "protocol ships it); per step the camera and settings go down and the RGBA8 image comes back"},
+        "kernels": kernels,
+    }
+    peaks = measured_peaks()
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import cpu
+
+        threads = os.cpu_count() or 1
+        from meercadraytracer_b200.compile import compile_scene
+
+        base = oracle_sample(compiled, cam, bench, args.cpu_seconds, threads)
+        bpq = bytes_per_query(base["counters"])
+        rays_k = k["closest_rays"] if top == "extend" else k["any_rays"]
+        per_launch_bytes = bpq["closest" if top == "extend" else "any"] * rays_k / max(1, kernels[top]["launches"])
+        avg_ms = kernels[top]["ms"] / max(1, kernels[top]["launches"])
+        achieved = per_launch_bytes / (avg_ms / 1000.0) / 1e9
+        line["roofline"] = {"bound": "hbm", "kernel": f"k_{top}", "achieved": round(achieved, 1),
+                            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
+                            "peak_source": peaks["source"], "traffic": traffic_from_profile(top),
+                            "bytes_per_query": round(bpq["closest" if top == "extend" else "any"], 1),
+                            "algorithmic_bytes_per_launch": round(per_launch_bytes)}
+        line["cpu_baseline"] = {"value": round(base["mrays_s"], 3), "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{base['pixels']} random pixels x {spp} passes ({base['rays']} rays, "
+                                          f"{base['seconds']:.1f} s) of the same workload on the oracle, a C++ "
+                                          f"restatement of the reference's TypeScript path (no Node.js here)"}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    ex.dispose()
+
+
+def traffic_from_profile(kernel: str) -> Optional[float]:
+    """DRAM bytes per launch of the kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    entry = d.get(f"k_{kernel}")
+    return None if entry is None else float(entry["bytes_per_launch_full_frame"])
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--config", choices=("mid", "small"), default="mid")
+    ap.add_argument("--capacity", type=int, default=0, help="path-state capacity (paths in flight)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="length of the CPU baseline sample")
+    ap.add_argument("--ref-seconds", type=float, default=10.0, help="length of each reference-arm step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be at least 3")
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,160 @@
+/*
+ * libmcrt: the C ABI of the B200 ray tracer.
+ *
+ * An mcrt_executor is one GPU tile executor: the device-side counterpart of
+ * the reference's worker (createTileHandler, src/protocol.ts:55-110, behind
+ * the TileExecutor interface of src/executors.ts:4-14). It keeps the latest
+ * geometry and shading it was sent, by version, and texture pixels by id, all
+ * resident in HBM, and renders tiles or whole images from them. A Node-API
+ * addon (or any FFI) binds these functions one to one; see INTEGRATION.md.
+ *
+ * Conventions: every function returns MCRT_OK (0) or an error code, and
+ * mcrt_last_error() then returns the message (per thread). Host pointers are
+ * borrowed for the duration of the call. Calls on one executor must not run
+ * concurrently; separate executors are independent.
+ */
+#ifndef MCRT_H
+#define MCRT_H
+
+#include <stdint.h>
+
+#include "mcrt_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCRT_OK 0
+#define MCRT_ERR_INVALID 1   /* bad argument or malformed scene data */
+#define MCRT_ERR_CUDA 2      /* a CUDA call failed */
+#define MCRT_ERR_NO_SCENE 3  /* geometry / shading version not received */
+#define MCRT_ERR_TEXTURE 4   /* a texture id was not sent */
+#define MCRT_ERR_LIMIT 5     /* beyond a documented limit */
+
+typedef struct mcrt_executor mcrt_executor;
+
+/* Work and device time of the renders since the last reset. */
+typedef struct mcrt_stats {
+  uint64_t closest_rays;  /* closest-hit BVH queries (camera and bounce rays) */
+  uint64_t any_rays;      /* any-hit BVH queries (shadow rays) */
+  uint64_t samples;       /* paths started */
+  uint64_t launches;      /* kernels launched */
+  double ms_total;        /* device time of whole render calls */
+  double ms_raygen, ms_extend, ms_shade, ms_shadow, ms_resolve, ms_accumulate;
+  uint64_t n_raygen, n_extend, n_shade, n_shadow, n_resolve, n_accumulate;
+  uint64_t path_bytes;    /* HBM held for path state */
+  uint64_t scene_bytes;   /* HBM held for the resident scene */
+  uint32_t status;        /* kernel-reported limits hit: 1 stack, 2 shadow list */
+  uint32_t pad_;
+} mcrt_stats;
+
+/* Message of the last failed call on this thread (empty after success). */
+const char* mcrt_last_error(void);
+
+/* ABI version: 1. */
+int32_t mcrt_version(void);
+
+/* Number of CUDA devices visible. */
+int32_t mcrt_device_count(int32_t* count);
+
+/* new WorkerExecutor(...) / createTileHandler(), src/executors.ts:54-94,
+ * src/protocol.ts:55: an executor on `device`. */
+int32_t mcrt_executor_create(int32_t device, mcrt_executor** out);
+
+/* TileExecutor.dispose, src/executors.ts:89-93. */
+int32_t mcrt_executor_destroy(mcrt_executor* executor);
+
+/* RequestMessage 'geometry', src/protocol.ts:30 and 64-67: replaces the
+ * resident geometry (CompiledGeometry with its BVH, src/types.ts:137-167). */
+int32_t mcrt_send_geometry(mcrt_executor* executor, int32_t version, const mcrt_geometry* geometry);
+
+/* RequestMessage 'textures', src/protocol.ts:31 and 68-70: texture pixels
+ * keyed by mcrt_texture.id, kept until the executor is destroyed. */
+int32_t mcrt_send_textures(mcrt_executor* executor, int32_t count, const mcrt_texture* items);
+
+/* RequestMessage 'shading', src/protocol.ts:32 and 71-74: materials, lights,
+ * environments, background and fog. A texture whose `data` is NULL refers
+ * to pixels sent before under its id. */
+int32_t mcrt_send_shading(mcrt_executor* executor, int32_t version, const mcrt_shading* shading);
+
+/* RequestMessage 'tile' answered by Tracer.renderTile (src/protocol.ts:75-104,
+ * src/tracer.ts:62-89): one pass of a tile, premultiplied RGBA floats,
+ * tile->width * tile->height * 4, row by row. Fails with MCRT_ERR_NO_SCENE
+ * when the versions are not the resident ones. */
+int32_t mcrt_render_tile(mcrt_executor* executor, int32_t geometry_version, int32_t shading_version,
+                         const mcrt_camera* camera, const mcrt_settings* settings, const mcrt_tile* tile,
+                         int32_t width, int32_t height, int32_t pass, int32_t block, float* out);
+
+/* raytraceCompiled, src/raytrace.ts:69-82, on the resident scene: `samples`
+ * passes, Float32 accumulation and RGBA8 encode on the device; out_rgba is a
+ * host buffer of width * height * 4 bytes, top row first, straight alpha. */
+int32_t mcrt_raytrace(mcrt_executor* executor, int32_t geometry_version, int32_t shading_version,
+                      const mcrt_camera* camera, const mcrt_settings* settings, int32_t width, int32_t height,
+                      int32_t samples, int32_t srgb, uint8_t* out_rgba);
+
+/* As mcrt_raytrace, writing into device memory (a CUDA device pointer of
+ * width * height * 4 bytes on the executor's device). */
+int32_t mcrt_raytrace_device(mcrt_executor* executor, int32_t geometry_version, int32_t shading_version,
+                             const mcrt_camera* camera, const mcrt_settings* settings, int32_t width,
+                             int32_t height, int32_t samples, int32_t srgb, void* device_rgba);
+
+/* raytraceCompiled restricted to listed pixels (each pixel is independent):
+ * out_rgba gets 4 bytes and out_sum (may be NULL) the 4 running-sum floats
+ * per listed pixel. */
+int32_t mcrt_render_pixels(mcrt_executor* executor, int32_t geometry_version, int32_t shading_version,
+                           const mcrt_camera* camera, const mcrt_settings* settings, int32_t width,
+                           int32_t height, int32_t samples, int32_t srgb, int32_t count, const int32_t* px,
+                           const int32_t* py, uint8_t* out_rgba, float* out_sum);
+
+/* The first closest-hit query of each listed pixel's sample for one pass:
+ * triangle index in BVH order (-1 for a miss), distance t and front flag. */
+int32_t mcrt_trace_primary(mcrt_executor* executor, int32_t geometry_version, const mcrt_camera* camera,
+                           int32_t width, int32_t height, int32_t pass, uint32_t seed, int32_t count,
+                           const int32_t* px, const int32_t* py, int32_t* triangle, float* t, int32_t* front);
+
+/* intersectClosest, src/bvh.ts:202-282, for `count` rays given as 8 floats
+ * each (origin xyz, -, direction xyz, -), culling by side when `cull`. */
+int32_t mcrt_intersect_closest(mcrt_executor* executor, int32_t geometry_version, int32_t count,
+                               const float* rays, int32_t cull, int32_t* triangle, float* t, float* u,
+                               int32_t* front);
+
+/* intersectAny, src/bvh.ts:289-332, with a counting visitor: the number of
+ * triangles each ray hits between 0 and its limit (rays as above, the 4th
+ * float a positive t limit or 0 for none). */
+int32_t mcrt_intersect_any_count(mcrt_executor* executor, int32_t geometry_version, int32_t count,
+                                 const float* rays, int32_t* counts);
+
+/* buildBvh, src/bvh.ts:16-178, on the GPU: binned SAH with 16 bins, leaves of
+ * at most 4 triangles (SAH leaves up to 16), depth at most 100. `bounds`
+ * and `nodes` hold max(1, 2 count - 1) nodes; *node_count receives the count. */
+int32_t mcrt_build_bvh(mcrt_executor* executor, const float* triangles, int32_t count, float* bounds,
+                       int32_t* nodes, uint32_t* order, int32_t* node_count);
+
+/* compileGeometry after the flatten, src/compile.ts:359-403, on the GPU:
+ * float32 rounding of world-space triangles, BVH, reorder into BVH order,
+ * tangents (writeTangent, src/compile.ts:406-432) and epsilon. Inputs and
+ * outputs as the reference's sink and CompiledGeometry (see oracle.h's
+ * oracle_compile_geometry for the same shapes). */
+int32_t mcrt_compile_geometry(mcrt_executor* executor, int32_t count, const double* p, const double* n,
+                              const double* uv, const double* colors, const uint8_t* has_color,
+                              const uint32_t* materials, const uint8_t* flags, const uint8_t* sides,
+                              float* triangles_out, float* normals_out, float* uvs_out, float* tangents_out,
+                              float* colors_out, uint32_t* materials_out, uint8_t* flags_out, uint8_t* sides_out,
+                              float* bounds_out, int32_t* nodes_out, uint32_t* order_out, int32_t* node_count_out,
+                              double* epsilon_out, int32_t* any_colors);
+
+/* Kernel timing with CUDA events on the executor's stream (adds a sync per
+ * kernel; for profiling only). */
+int32_t mcrt_set_timing(mcrt_executor* executor, int32_t enabled);
+
+/* Path-state capacity (paths in flight per launch); the autotuner sets it. */
+int32_t mcrt_set_capacity(mcrt_executor* executor, int32_t paths);
+
+int32_t mcrt_get_stats(mcrt_executor* executor, mcrt_stats* out);
+int32_t mcrt_reset_stats(mcrt_executor* executor);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCRT_H */

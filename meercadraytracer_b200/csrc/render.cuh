@@ -1,0 +1,129 @@
+// Host-side interface of the wavefront renderer (render.cu) and the device
+// path-state layout its kernels share.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "device_scene.cuh"
+
+namespace mcrt {
+
+// Per-path flag bits.
+constexpr uint32_t kFlagSeen = 1u;       // surfaceSeen, tracer.ts:102
+constexpr uint32_t kFlagToneMap = 2u;    // toneMapped, tracer.ts:103
+constexpr uint32_t kFlagCull = 4u;       // cull, tracer.ts:109
+constexpr uint32_t kFlagDone = 8u;       // the path loop ended; finalize after this bounce's shadows
+constexpr uint32_t kFlagDirect = 16u;    // the sample was written directly (a background)
+MCRT_HD uint32_t flag_passes(uint32_t f) { return (f >> 8) & 0xffu; }
+MCRT_HD uint32_t flag_bounce(uint32_t f) { return (f >> 16) & 0xffu; }
+MCRT_HD int flag_last_env(uint32_t f) { return static_cast<int>(f >> 24) - 1; }
+
+// Camera, image, sample mapping and settings of one launch series.
+struct FrameParams {
+  double proj_inv[16];
+  double world[16];
+  float cam_forward[3];
+  float cam_position[3];
+  int width, height;
+  int pass0;       // pass of the first slice of paths
+  int npix;        // paths per pass in this launch series: pixels, blocks, or listed pixels
+  int pix0;        // index of the first of them in the tile / block grid / pixel list
+  int mode;        // 0: tile grid (with block), 1: pixel list
+  int tile_x, tile_y, tile_w, tile_h, block, nbx;
+  const int* list_x;
+  const int* list_y;
+  uint32_t seed;
+  int max_bounces, shadows, gi, tone_mapping;
+  float exposure;
+  float clear_color[3], clear_alpha;
+  int slot_count;  // shadow slots per path: lights + 1
+  int capacity;    // path-state capacity
+};
+
+// Structure-of-arrays path state, indexed by path id.
+struct PathState {
+  float4* ray_o;   // origin, -
+  float4* ray_d;   // direction, -
+  float4* hit;     // t, u, v, bits((front << 31) | (triangle + 1)); 0 = miss
+  float4* thr;     // throughput rgb, fog factor
+  float4* rad;     // radiance rgb, last environment scale
+  float4* med;     // absorption rgb of the volume the ray is in, -
+  uint32_t* rng;
+  uint32_t* flags;
+  unsigned long long* smask;  // shadow slots written this bounce
+  float4* sample;  // finished sample: premultiplied, tone mapped RGBA
+  float4* slots;   // [slot][capacity] shadow contributions
+  int* queue[2];
+  float4* shadow_queue;  // 3 float4 per shadow ray
+};
+
+struct Counters {
+  unsigned int next_count;
+  unsigned int shadow_count;
+  unsigned int status;
+  unsigned int pad;
+};
+
+// Work and time of the kernels of one render, for benchmarks.
+struct RenderStats {
+  unsigned long long closest_rays = 0;
+  unsigned long long any_rays = 0;
+  unsigned long long samples = 0;
+  unsigned long long launches = 0;
+  double ms_raygen = 0, ms_extend = 0, ms_shade = 0, ms_shadow = 0, ms_resolve = 0, ms_accumulate = 0;
+  unsigned long long n_raygen = 0, n_extend = 0, n_shade = 0, n_shadow = 0, n_resolve = 0, n_accumulate = 0;
+  unsigned int status = 0;
+};
+
+// Device buffers of the path state, grown on demand.
+class PathBuffers {
+ public:
+  ~PathBuffers();
+  // Makes room for `capacity` paths with `slots` shadow slots each.
+  cudaError_t reserve(int capacity, int slots);
+  PathState state() const { return st_; }
+  int capacity() const { return capacity_; }
+  int slots() const { return slots_; }
+  size_t bytes() const { return bytes_; }
+  Counters* counters() const { return counters_; }
+  Counters* host_counters() const { return host_counters_; }
+
+ private:
+  void release();
+  PathState st_{};
+  Counters* counters_ = nullptr;
+  Counters* host_counters_ = nullptr;
+  std::vector<void*> allocations_;
+  int capacity_ = 0;
+  int slots_ = 0;
+  size_t bytes_ = 0;
+};
+
+// Traces `passes` passes over `npix` paths per pass (pixels, blocks or listed
+// pixels as `fp` maps them), in chunks of at most the buffers' capacity,
+// calling `on_chunk(first_pass, pass_count)` after each chunk so the caller
+// can consume the samples. Returns a CUDA error, or cudaSuccess.
+class Wavefront {
+ public:
+  cudaError_t run(const DScene& scene, FrameParams fp, int passes, PathBuffers& buffers, cudaStream_t stream,
+                  RenderStats* stats, bool timed,
+                  cudaError_t (*on_chunk)(void* ctx, int first_pass, int pass_count), void* ctx);
+};
+
+// Camera rays of one pass over fp.npix paths and their closest hits, left in
+// the path state's `hit` array.
+cudaError_t primary_hits(const DScene& scene, FrameParams fp, PathBuffers& buffers, cudaStream_t stream);
+
+// Kernel launchers used by the executor.
+cudaError_t launch_accumulate(const float4* samples, int npix, int passes_in_chunk, float4* sum, int total_passes,
+                              int last_chunk, uint8_t* image, const FrameParams& fp, int srgb, cudaStream_t s);
+cudaError_t launch_tile_output(const float4* samples, const FrameParams& fp, float* out, cudaStream_t s);
+cudaError_t launch_trace_rays(const DScene& scene, const float4* rays, int count, int cull, int4* hits,
+                              cudaStream_t s);
+cudaError_t launch_count_hits(const DScene& scene, const float4* rays, int count, int* counts, cudaStream_t s);
+
+}  // namespace mcrt

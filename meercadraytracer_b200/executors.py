@@ -1,0 +1,335 @@
+"""The GPU tile executor: the TileExecutor interface of src/executors.ts:4-14
+backed by an executor of libmcrt (include/mcrt.h) on one CUDA device.
+
+Messages are the reference's RequestMessage (src/protocol.ts:29-45) as dicts
+with snake_case keys:
+
+  {"type": "geometry", "version": v, "geometry": CompiledGeometry}
+  {"type": "textures", "items": [{"id": i, "data": ndarray}, ...]}
+  {"type": "shading", "version": v, "shading": ShadingPayload}
+  {"type": "tile", "job": j, "geometry_version": g, "shading_version": s,
+   "camera": CompiledCamera, "settings": TraceSettings, "tile": Tile,
+   "width": w, "height": h, "pass": p, "block": b}
+
+`render` resolves with the tile's premultiplied RGBA float32 samples, as the
+worker's Tracer.renderTile does; a tile that refers to a scene the executor
+has not received, or any GPU failure, rejects it with an Error, as
+createTileHandler answers {type: 'error'} (src/protocol.ts:75-104). There is
+no CPU fallback: failures surface to the caller.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from concurrent.futures import Future, ThreadPoolExecutor
+from dataclasses import dataclass, field
+from typing import Any, Dict, List, Optional, Sequence, Set, Tuple
+
+import numpy as np
+
+from . import abi
+from ._lib import McrtError, call, load, mcrt_stats
+from .types import (
+    CompiledBvh,
+    CompiledCamera,
+    CompiledGeometry,
+    CompiledScene,
+    CompiledTexture,
+    Tile,
+    TraceSettings,
+)
+
+
+@dataclass
+class ShadingPayload:
+    """ShadingPayload, src/protocol.ts:19-27: everything but geometry and texture pixels."""
+
+    materials: list
+    textures: list  # CompiledTexture metadata; `texture_ids[i]` names the pixels of textures[i]
+    texture_ids: List[int]
+    environments: list
+    lights: list
+    background: Any
+    environment: int
+    fog: Any
+
+    @staticmethod
+    def of(scene: CompiledScene, texture_ids: Sequence[int]) -> "ShadingPayload":
+        return ShadingPayload(scene.materials, scene.textures, list(texture_ids), scene.environments, scene.lights,
+                              scene.background, scene.environment, scene.fog)
+
+
+class GpuExecutor:
+    """One CUDA device as a TileExecutor: the scene stays resident in HBM."""
+
+    # One render at a time per executor: whole frames already fill the GPU.
+    concurrency = 1
+
+    def __init__(self, device: int = 0):
+        load()
+        handle = C.c_void_p()
+        call("mcrt_executor_create", int(device), C.byref(handle))
+        self._h = handle
+        self.device = device
+        self.textures: Set[int] = set()  # texture ids this executor holds (TileExecutor.textures)
+        self._pending_pixels: Dict[int, np.ndarray] = {}
+        self._lock = threading.Lock()
+        self._worker = ThreadPoolExecutor(max_workers=1, thread_name_prefix=f"mcrt{device}")
+        self._disposed = False
+        self._geometry_version: Optional[int] = None
+        self._shading_version: Optional[int] = None
+        self._versions = 0
+        self._scene_ref: Optional[CompiledScene] = None
+        self._geometry_ref: Optional[CompiledGeometry] = None
+        self._slots: Tuple[int, int] = (0, 0)
+
+    # ------------------------------------------------------------ messages
+    def send(self, message: Dict[str, Any], transfer: Any = None) -> None:
+        """TileExecutor.send: messages are processed in the order they are sent."""
+        self._check()
+        kind = message["type"]
+        with self._lock:
+            if kind == "geometry":
+                g, keep = abi.to_c_geometry(message["geometry"])
+                call("mcrt_send_geometry", self._h, int(message["version"]), C.byref(g))
+                self._geometry_version = int(message["version"])
+            elif kind == "textures":
+                for item in message["items"]:
+                    self._pending_pixels[int(item["id"])] = item["data"]
+                    self.textures.add(int(item["id"]))
+            elif kind == "shading":
+                sh: ShadingPayload = message["shading"]
+                self._send_shading(int(message["version"]), sh)
+            else:
+                raise ValueError(f"unknown message type {kind!r}")
+
+    def _send_shading(self, version: int, sh: ShadingPayload) -> None:
+        scene = CompiledScene(geometry=None, materials=sh.materials, textures=[], environments=sh.environments,  # type: ignore[arg-type]
+                              lights=sh.lights, background=sh.background, environment=sh.environment, fog=sh.fog)
+        s, keep = abi.to_c_shading(scene)
+        arr = (abi.mcrt_texture * max(1, len(sh.textures)))()
+        fresh = []
+        for i, (t, tid) in enumerate(zip(sh.textures, sh.texture_ids)):
+            # Pixels travel once per executor (src/progressive.ts:140-148); a
+            # texture without them here refers to pixels uploaded before.
+            data = self._pending_pixels.get(tid)
+            meta = CompiledTexture(t.width, t.height, data if data is not None else t.data, t.srgb, t.flip_y,
+                                   t.wrap_s, t.wrap_t, t.matrix)
+            arr[i], k = abi.to_c_texture(meta, tid, with_data=data is not None)
+            keep.extend(k)
+            if data is not None:
+                fresh.append(tid)
+        s.texture_count = len(sh.textures)
+        s.textures = arr
+        keep.append(arr)
+        call("mcrt_send_shading", self._h, version, C.byref(s))
+        for tid in fresh:
+            self._pending_pixels.pop(tid, None)
+        self._shading_version = version
+
+    def render(self, message: Dict[str, Any]) -> "Future[np.ndarray]":
+        """TileExecutor.render: resolves with the tile's premultiplied RGBA floats."""
+        fut: Future = Future()
+        if self._disposed:
+            fut.set_exception(RuntimeError("the renderer was disposed"))
+            return fut
+        return self._worker.submit(self._render_tile, message)
+
+    def _render_tile(self, m: Dict[str, Any]) -> np.ndarray:
+        tile: Tile = m["tile"]
+        out = np.zeros(tile.width * tile.height * 4, np.float32)
+        cam = abi.to_c_camera(m["camera"])
+        st = abi.to_c_settings(m["settings"])
+        t = abi.to_c_tile(tile)
+        with self._lock:
+            call("mcrt_render_tile", self._h, int(m["geometry_version"]), int(m["shading_version"]), C.byref(cam),
+                 C.byref(st), C.byref(t), int(m["width"]), int(m["height"]), int(m["pass"]), int(m.get("block", 1)),
+                 abi.ptr(out, C.c_float))
+        return out
+
+    def dispose(self) -> None:
+        """TileExecutor.dispose: frees the device state."""
+        if self._disposed:
+            return
+        self._disposed = True
+        self._worker.shutdown(wait=True)
+        call("mcrt_executor_destroy", self._h)
+        self._h = None
+
+    def __del__(self):  # pragma: no cover - best effort
+        try:
+            if not self._disposed and self._h is not None:
+                self.dispose()
+        except Exception:
+            pass
+
+    def _check(self) -> None:
+        if self._disposed:
+            raise RuntimeError("the renderer was disposed")
+
+    # ---------------------------------------------------- whole-scene calls
+    def load_scene(self, scene: CompiledScene) -> Tuple[int, int]:
+        """Makes `scene` resident (geometry, texture pixels, shading) unless it already is."""
+        self._check()
+        # Hold the scene itself: comparing id()s alone could match a new scene
+        # allocated where a freed one was.
+        if self._scene_ref is scene and self._geometry_ref is scene.geometry and self._geometry_version is not None:
+            return self._slots
+        self._versions += 1
+        gv = sv = self._versions
+        self.send({"type": "geometry", "version": gv, "geometry": scene.geometry})
+        ids = [self._versions * 100000 + i for i in range(len(scene.textures))]
+        self.send({"type": "textures", "items": [{"id": i, "data": t.data} for i, t in zip(ids, scene.textures)]})
+        self.send({"type": "shading", "version": sv, "shading": ShadingPayload.of(scene, ids)})
+        self._scene_ref = scene
+        self._geometry_ref = scene.geometry
+        self._slots = (gv, sv)
+        return gv, sv
+
+    def raytrace(self, scene: CompiledScene, camera: CompiledCamera, width: int, height: int,
+                 settings: TraceSettings, samples: int = 16, srgb: bool = True) -> np.ndarray:
+        """raytraceCompiled (src/raytrace.ts:69-82) on the device: RGBA8 bytes."""
+        gv, sv = self.load_scene(scene)
+        out = np.zeros(width * height * 4, np.uint8)
+        cam, st = abi.to_c_camera(camera), abi.to_c_settings(settings)
+        with self._lock:
+            call("mcrt_raytrace", self._h, gv, sv, C.byref(cam), C.byref(st), int(width), int(height), int(samples),
+                 int(bool(srgb)), abi.ptr(out, C.c_uint8))
+        return out
+
+    def raytrace_device(self, scene: CompiledScene, camera: CompiledCamera, width: int, height: int,
+                        settings: TraceSettings, samples: int, srgb: bool, device_ptr: int) -> None:
+        """As raytrace, leaving the image in device memory at `device_ptr`."""
+        gv, sv = self.load_scene(scene)
+        cam, st = abi.to_c_camera(camera), abi.to_c_settings(settings)
+        with self._lock:
+            call("mcrt_raytrace_device", self._h, gv, sv, C.byref(cam), C.byref(st), int(width), int(height),
+                 int(samples), int(bool(srgb)), C.c_void_p(device_ptr))
+
+    def render_pixels(self, scene: CompiledScene, camera: CompiledCamera, width: int, height: int,
+                      settings: TraceSettings, samples: int, srgb: bool, px: np.ndarray, py: np.ndarray
+                      ) -> Tuple[np.ndarray, np.ndarray]:
+        """raytraceCompiled for listed pixels: (rgba uint8 [n, 4], sums float32 [n, 4])."""
+        gv, sv = self.load_scene(scene)
+        px = np.ascontiguousarray(px, np.int32)
+        py = np.ascontiguousarray(py, np.int32)
+        n = px.size
+        rgba = np.zeros(n * 4, np.uint8)
+        sums = np.zeros(n * 4, np.float32)
+        cam, st = abi.to_c_camera(camera), abi.to_c_settings(settings)
+        with self._lock:
+            call("mcrt_render_pixels", self._h, gv, sv, C.byref(cam), C.byref(st), int(width), int(height),
+                 int(samples), int(bool(srgb)), n, abi.ptr(px, C.c_int32), abi.ptr(py, C.c_int32),
+                 abi.ptr(rgba, C.c_uint8), abi.ptr(sums, C.c_float))
+        return rgba.reshape(n, 4), sums.reshape(n, 4)
+
+    def trace_primary(self, scene: CompiledScene, camera: CompiledCamera, width: int, height: int, pass_: int,
+                      seed: float, px: np.ndarray, py: np.ndarray) -> Dict[str, np.ndarray]:
+        gv, _ = self.load_scene(scene)
+        px = np.ascontiguousarray(px, np.int32)
+        py = np.ascontiguousarray(py, np.int32)
+        n = px.size
+        tri = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        front = np.zeros(n, np.int32)
+        cam = abi.to_c_camera(camera)
+        with self._lock:
+            call("mcrt_trace_primary", self._h, gv, C.byref(cam), int(width), int(height), int(pass_),
+                 abi.to_uint32(seed), n, abi.ptr(px, C.c_int32), abi.ptr(py, C.c_int32), abi.ptr(tri, C.c_int32),
+                 abi.ptr(t, C.c_float), abi.ptr(front, C.c_int32))
+        return {"tri": tri, "t": t, "front": front}
+
+    def intersect_closest(self, geometry_version: int, rays: np.ndarray, cull: bool = True
+                          ) -> Dict[str, np.ndarray]:
+        """intersectClosest for rays [n, 8] (origin, -, direction, -) on the resident geometry."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        tri = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        u = np.zeros(n, np.float32)
+        front = np.zeros(n, np.int32)
+        with self._lock:
+            call("mcrt_intersect_closest", self._h, int(geometry_version), n, abi.ptr(rays, C.c_float), int(cull),
+                 abi.ptr(tri, C.c_int32), abi.ptr(t, C.c_float), abi.ptr(u, C.c_float), abi.ptr(front, C.c_int32))
+        return {"tri": tri, "t": t, "u": u, "front": front}
+
+    def intersect_any_count(self, geometry_version: int, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        counts = np.zeros(n, np.int32)
+        with self._lock:
+            call("mcrt_intersect_any_count", self._h, int(geometry_version), n, abi.ptr(rays, C.c_float),
+                 abi.ptr(counts, C.c_int32))
+        return counts
+
+    # ------------------------------------------------------------ compile
+    def build_bvh(self, triangles: np.ndarray, count: int) -> Tuple[CompiledBvh, np.ndarray]:
+        """buildBvh (src/bvh.ts:16-178) on the GPU."""
+        tris = np.ascontiguousarray(triangles, np.float32)
+        cap = max(1, 2 * count - 1)
+        bounds = np.zeros(cap * 6, np.float32)
+        nodes = np.zeros(cap * 3, np.int32)
+        order = np.zeros(max(1, count), np.uint32)
+        m = C.c_int32()
+        with self._lock:
+            call("mcrt_build_bvh", self._h, abi.ptr(tris, C.c_float), int(count), abi.ptr(bounds, C.c_float),
+                 abi.ptr(nodes, C.c_int32), abi.ptr(order, C.c_uint32), C.byref(m))
+        k = int(m.value)
+        return CompiledBvh(bounds[: k * 6].copy(), nodes[: k * 3].copy(), k), order[:count].copy()
+
+    def compile_sink(self, sink: Any) -> CompiledGeometry:
+        """compileGeometry after the flatten (src/compile.ts:359-403) on the GPU."""
+        n = sink.count
+        cap = max(1, 2 * n - 1)
+        f32, u8, u32 = np.float32, np.uint8, np.uint32
+        tris, nrm = np.zeros(n * 9, f32), np.zeros(n * 9, f32)
+        uvs, tan = np.zeros(n * 6, f32), np.zeros(n * 4, f32)
+        colors = np.zeros(max(1, n * 12), f32)
+        mats, flags, sides = np.zeros(n, u32), np.zeros(n, u8), np.zeros(n, u8)
+        bounds, nodes, order = np.zeros(cap * 6, f32), np.zeros(cap * 3, np.int32), np.zeros(max(1, n), u32)
+        node_count, eps, any_colors = C.c_int32(), C.c_double(), C.c_int32()
+        c = lambda a, dt: np.ascontiguousarray(a, dt)  # noqa: E731
+        p, nn, uv, col = c(sink.p, np.float64), c(sink.n, np.float64), c(sink.uv, np.float64), c(sink.colors, np.float64)
+        hc, sm, sf, ss = c(sink.has_color, u8), c(sink.materials, u32), c(sink.flags, u8), c(sink.sides, u8)
+        P, D = abi.ptr, C.c_double
+        with self._lock:
+            call("mcrt_compile_geometry", self._h, n, P(p, D), P(nn, D), P(uv, D), P(col, D), P(hc, C.c_uint8),
+                 P(sm, C.c_uint32), P(sf, C.c_uint8), P(ss, C.c_uint8), P(tris, C.c_float), P(nrm, C.c_float),
+                 P(uvs, C.c_float), P(tan, C.c_float), P(colors, C.c_float), P(mats, C.c_uint32), P(flags, C.c_uint8),
+                 P(sides, C.c_uint8), P(bounds, C.c_float), P(nodes, C.c_int32), P(order, C.c_uint32),
+                 C.byref(node_count), C.byref(eps), C.byref(any_colors))
+        m = int(node_count.value)
+        return CompiledGeometry(
+            triangle_count=n, triangles=tris, normals=nrm, uvs=uvs, tangents=tan,
+            colors=colors[: n * 12].copy() if any_colors.value else np.zeros(0, f32), materials=mats, flags=flags,
+            sides=sides, bvh=CompiledBvh(bounds[: m * 6].copy(), nodes[: m * 3].copy(), m), epsilon=float(eps.value),
+            order=order[:n].copy())
+
+    # -------------------------------------------------------------- tuning
+    def set_timing(self, enabled: bool) -> None:
+        call("mcrt_set_timing", self._h, int(bool(enabled)))
+
+    def set_capacity(self, paths: int) -> None:
+        call("mcrt_set_capacity", self._h, int(paths))
+
+    def stats(self) -> Dict[str, Any]:
+        s = mcrt_stats()
+        call("mcrt_get_stats", self._h, C.byref(s))
+        return s.as_dict()
+
+    def reset_stats(self) -> None:
+        call("mcrt_reset_stats", self._h)
+
+
+_default: Dict[int, GpuExecutor] = {}
+_default_lock = threading.Lock()
+
+
+def default_executor(device: int = 0) -> GpuExecutor:
+    """A process-wide executor per device, created on first use."""
+    with _default_lock:
+        ex = _default.get(device)
+        if ex is None or ex._disposed:
+            ex = GpuExecutor(device)
+            _default[device] = ex
+        return ex

@@ -1,0 +1,232 @@
+"""Seeded synthetic scenes of the benchmark configurations.
+
+No public dataset is involved: every scene is generated from a fixed seed
+(0x5EED0000 + configuration index) with the shapes, sizes and value
+distributions the configurations name. Placements the configurations leave
+open (light positions, camera of the mid scene, ground material) are fixed
+here and documented in DESIGN.md.
+
+  small_scene()  22,530 triangles: a 40 x 40 ground plane and 64 UV spheres
+                 (16 x 12 segments), 320 x 240, 16 spp, GI off, ACES, sRGB.
+  mid_scene()    1,310,720 triangles: 256 icospheres subdivided 4 times
+                 (5,120 triangles each) displaced by value noise on a 16 x 16
+                 grid, mixed Standard / Physical / Phong materials, half with
+                 256 x 256 noise albedo maps; 1920 x 1080, 64 spp, GI on,
+                 4 bounces, ACES, sRGB.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Any, Dict, List, Tuple
+
+import numpy as np
+
+from . import scene as S
+
+SEED_BASE = 0x5EED0000
+
+
+@dataclass
+class BenchScene:
+    """A scene description, its camera, image size and raytrace options."""
+
+    name: str
+    scene: S.Scene
+    camera: S.Camera
+    width: int
+    height: int
+    options: Dict[str, Any] = field(default_factory=dict)
+    triangles: int = 0
+
+
+def _srgb_color(rgb: np.ndarray) -> S.Color:
+    """An sRGB-encoded colour decoded to linear, as three.js's setRGB(..., SRGBColorSpace) does."""
+    return S.Color(S.srgb_to_linear(float(rgb[0])), S.srgb_to_linear(float(rgb[1])), S.srgb_to_linear(float(rgb[2])))
+
+
+def small_scene(seed: int = SEED_BASE + 0) -> BenchScene:
+    """The small plain-method scene (a few thousand lines of three.js in the reference's terms)."""
+    rng = np.random.default_rng(seed)
+    scene = S.Scene()
+    ground = S.Mesh(S.plane_geometry(40, 40), S.MeshStandardMaterial(color=S.Color(0.5, 0.5, 0.5), roughness=0.9))
+    ground.rotation.x = -math.pi / 2
+    scene.add(ground)
+    count = 0
+    for _ in range(64):
+        r = float(rng.uniform(0.3, 1.2))
+        x, z = float(rng.uniform(-8, 8)), float(rng.uniform(-8, 8))
+        colour = rng.uniform(0, 1, 3)
+        material = S.MeshStandardMaterial(color=_srgb_color(colour), roughness=float(rng.uniform(0.05, 1)),
+                                          metalness=float(rng.integers(0, 2)))
+        sphere = S.Mesh(S.sphere_geometry(r, 16, 12), material)
+        sphere.position.set(x, r, z)
+        scene.add(sphere)
+        count += 352
+    sun = S.DirectionalLight(0xffffff, 3)
+    sun.position.set(5, 10, 7)
+    sun.cast_shadow = True
+    lamp = S.PointLight(0xffffff, 50, 0)
+    lamp.position.set(-4, 6, 4)
+    scene.add(sun, lamp)
+    camera = S.PerspectiveCamera(50, 320 / 240, 0.1, 2000)
+    camera.position.set(0, 6, 16)
+    camera.look_at(0, 0, 0)
+    camera.update_matrix_world()
+    return BenchScene("small: 64 UV spheres + ground, 22,530 tris, 320x240, 16 spp, GI off", scene, camera, 320, 240,
+                      {"samples": 16, "global_illumination": False, "tone_mapping": S.ACESFilmicToneMapping,
+                       "output_color_space": "srgb", "max_bounces": 4}, count + 2)
+
+
+# ------------------------------------------------------------- icospheres
+def icosphere(subdivisions: int) -> Tuple[np.ndarray, np.ndarray]:
+    """Unit icosphere: an icosahedron whose faces are split in four `subdivisions`
+    times, new vertices pushed to the sphere. Returns (vertices [v, 3], faces [f, 3])."""
+    t = (1 + math.sqrt(5)) / 2
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+             (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    v = np.array(verts, np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array(faces, np.int64)
+    for _ in range(subdivisions):
+        edges = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        key = np.sort(edges, axis=1)
+        uniq, inverse = np.unique(key, axis=0, return_inverse=True)
+        mids = v[uniq[:, 0]] + v[uniq[:, 1]]
+        mids /= np.linalg.norm(mids, axis=1, keepdims=True)
+        base = v.shape[0]
+        v = np.concatenate([v, mids])
+        m = inverse.reshape(3, -1).T + base  # midpoints of edges 01, 12, 20
+        a, b, c = f[:, 0], f[:, 1], f[:, 2]
+        ab, bc, ca = m[:, 0], m[:, 1], m[:, 2]
+        f = np.concatenate([np.stack([a, ab, ca], 1), np.stack([b, bc, ab], 1), np.stack([c, ca, bc], 1),
+                            np.stack([ab, bc, ca], 1)])
+    return v, f
+
+
+def _lattice_hash(ix: np.ndarray, iy: np.ndarray, iz: np.ndarray, seed: int) -> np.ndarray:
+    """A value in [0, 1) per integer lattice point (lowbias32-style integer mix)."""
+    h = (ix.astype(np.int64) * 73856093) ^ (iy.astype(np.int64) * 19349663) ^ (iz.astype(np.int64) * 83492791)
+    h = (h ^ seed) & 0xFFFFFFFF
+    h ^= h >> 16
+    h = (h * 0x7FEB352D) & 0xFFFFFFFF
+    h ^= h >> 15
+    h = (h * 0x846CA68B) & 0xFFFFFFFF
+    h ^= h >> 16
+    return h.astype(np.float64) / 4294967296.0
+
+
+def value_noise3(p: np.ndarray, seed: int) -> np.ndarray:
+    """Smoothly interpolated lattice value noise in [0, 1) at points p [n, 3]."""
+    f = np.floor(p)
+    i = f.astype(np.int64)
+    t = p - f
+    w = t * t * (3 - 2 * t)
+    out = np.zeros(p.shape[0])
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                h = _lattice_hash(i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz, seed)
+                wx = w[:, 0] if dx else 1 - w[:, 0]
+                wy = w[:, 1] if dy else 1 - w[:, 1]
+                wz = w[:, 2] if dz else 1 - w[:, 2]
+                out += h * wx * wy * wz
+    return out
+
+
+def noise_texture(size: int, seed: int) -> np.ndarray:
+    """size x size RGBA8 value-noise image: two octaves of smoothly interpolated
+    seeded lattice values per colour channel, opaque."""
+    rng = np.random.default_rng(seed)
+    img = np.zeros((size, size, 3))
+    coords = np.arange(size) / 32.0
+    for freq, amp in ((1.0, 0.65), (2.7, 0.35)):
+        c = coords * freq
+        i = np.floor(c).astype(np.int64)
+        t = c - i
+        w = t * t * (3 - 2 * t)
+        n = int(i.max()) + 2
+        for ch in range(3):
+            g = rng.uniform(0, 1, (n, n))
+            v = (g[np.ix_(i, i)] * np.outer(1 - w, 1 - w) + g[np.ix_(i, i + 1)] * np.outer(1 - w, w) +
+                 g[np.ix_(i + 1, i)] * np.outer(w, 1 - w) + g[np.ix_(i + 1, i + 1)] * np.outer(w, w))
+            img[:, :, ch] += amp * v
+    out = np.empty((size, size, 4), np.uint8)
+    out[:, :, :3] = np.clip(img * 255 + 0.5, 0, 255).astype(np.uint8)
+    out[:, :, 3] = 255
+    return out.reshape(-1)
+
+
+def displaced_icosphere(subdivisions: int, amplitude: float, seed: int) -> S.BufferGeometry:
+    """An icosphere whose radius is 1 + amplitude * (noise - 0.5), with smooth
+    normals from the displaced faces and spherical uvs."""
+    v, f = icosphere(subdivisions)
+    r = 1 + amplitude * (value_noise3(v * 3.0 + 11.0, seed) - 0.5)
+    p = v * r[:, None]
+    e1 = p[f[:, 1]] - p[f[:, 0]]
+    e2 = p[f[:, 2]] - p[f[:, 0]]
+    fn = np.cross(e1, e2)
+    n = np.zeros_like(p)
+    for k in range(3):
+        np.add.at(n, f[:, k], fn)
+    n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30)
+    uv = np.stack([np.arctan2(v[:, 2], v[:, 0]) / (2 * math.pi) + 0.5, np.arcsin(np.clip(v[:, 1], -1, 1)) / math.pi + 0.5],
+                  axis=1)
+    return S.BufferGeometry(p.astype(np.float32), n.astype(np.float32), uv.astype(np.float32),
+                            index=f.reshape(-1).astype(np.uint32))
+
+
+def mid_scene(seed: int = SEED_BASE + 1, grid: int = 16, subdivisions: int = 4, width: int = 1920,
+              height: int = 1080, samples: int = 64) -> BenchScene:
+    """The path-traced mid scene: grid x grid displaced icospheres."""
+    rng = np.random.default_rng(seed)
+    scene = S.Scene()
+    spacing = 5.0
+    textures: List[S.DataTexture] = []
+    count = 0
+    for gz in range(grid):
+        for gx in range(grid):
+            k = gz * grid + gx
+            geometry = displaced_icosphere(subdivisions, 0.1, seed + k)
+            kind = rng.uniform()
+            if kind < 0.4:
+                material: S.Material = S.MeshStandardMaterial(roughness=float(rng.uniform(0, 1)),
+                                                              metalness=float(rng.uniform(0, 1)))
+            elif kind < 0.7:
+                material = S.MeshPhysicalMaterial(transmission=1.0, ior=1.5, roughness=float(rng.uniform(0, 0.2)))
+            else:
+                material = S.MeshPhongMaterial(shininess=float(rng.uniform(1, 200)))
+            material.color = _srgb_color(rng.uniform(0.2, 1.0, 3))
+            if rng.uniform() < 0.5:
+                tex = S.DataTexture(noise_texture(256, seed + 1000 + k), 256, 256)
+                tex.color_space = S.SRGBColorSpace
+                tex.wrap_s = tex.wrap_t = S.RepeatWrapping
+                material.map = tex
+                textures.append(tex)
+            mesh = S.Mesh(geometry, material)
+            s = float(rng.uniform(0.5, 2.0))
+            mesh.scale.set(s, s, s)
+            mesh.position.set((gx - (grid - 1) / 2) * spacing, s, (gz - (grid - 1) / 2) * spacing)
+            scene.add(mesh)
+            count += f_count(subdivisions)
+    half = grid * spacing / 2
+    for sx, sz in ((-1, -1), (-1, 1), (1, -1), (1, 1)):
+        light = S.PointLight(0xffffff, 2500.0, 0, 2)
+        light.position.set(sx * half * 0.5, 40.0, sz * half * 0.5)
+        scene.add(light)
+    scene.add(S.HemisphereLight(0xddeeff, 0x202020, 0.5))
+    camera = S.PerspectiveCamera(50, width / height, 0.1, 2000)
+    camera.position.set(0, 32, 62)
+    camera.look_at(0, 0, 0)
+    camera.update_matrix_world()
+    return BenchScene(f"mid: {grid * grid} displaced icospheres, {count:,} tris, {width}x{height}, {samples} spp, GI on",
+                      scene, camera, width, height,
+                      {"samples": samples, "global_illumination": True, "max_bounces": 4,
+                       "tone_mapping": S.ACESFilmicToneMapping, "output_color_space": "srgb"}, count)
+
+
+def f_count(subdivisions: int) -> int:
+    return 20 * 4 ** subdivisions

@@ -1,0 +1,260 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle.
+
+Criteria, from the reference's own tests and the stated accuracy targets:
+  * BVH: the GPU build makes the reference's split decisions, so both trees
+    group the same triangles (compared as canonical trees of original ids).
+  * Closest hits: same triangle as brute force / the oracle on >= 99.99 % of
+    rays, the rest ties (same distance within 1e-5 relative); t within 1e-5
+    relative.
+  * Deterministic renders: RGBA8 within +-1 level on >= 99.9 % of pixels.
+  * Same inputs give the same bytes.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from meercadraytracer_b200 import scene as S
+from meercadraytracer_b200._lib import McrtError
+from meercadraytracer_b200.compile import compile_camera, compile_scene, flatten_meshes, compile_shading
+from meercadraytracer_b200.executors import GpuExecutor
+from meercadraytracer_b200.raytrace import as_options, output_srgb, sample_count, trace_settings
+from meercadraytracer_b200 import scenes
+from oracle import cpu
+
+from test_oracle_bvh_color import brute_force, lcg_triangles, lissajous_ray, reorder
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    ex = GpuExecutor(0)
+    yield ex
+    ex.dispose()
+
+
+def canonical(bvh, order, node=0):
+    """A node as a comparable value: leaves by their set of original triangle ids."""
+    nodes = bvh.nodes.reshape(-1, 3)
+    first, count, axis = (int(x) for x in nodes[node])
+    if count > 0:
+        return frozenset(int(order[k]) for k in range(first, first + count))
+    return (axis, canonical(bvh, order, first), canonical(bvh, order, first + 1))
+
+
+def leaf_sets(bvh, order):
+    nodes = bvh.nodes.reshape(-1, 3)
+    return sorted(tuple(sorted(int(order[k]) for k in range(f, f + c))) for f, c, _ in nodes if c > 0)
+
+
+# ------------------------------------------------------------------- BVH build
+@pytest.mark.parametrize("count,seed", [(3000, 7), (20000, 11), (5, 3), (17, 4), (1, 1)])
+def test_gpu_bvh_matches_oracle(gpu, count, seed):
+    raw = lcg_triangles(count, seed)
+    ob, oo = cpu.build_bvh(raw, count)
+    gb, go = gpu.build_bvh(raw, count)
+    assert gb.node_count == ob.node_count
+    assert sorted(go.tolist()) == list(range(count))
+    assert canonical(gb, go) == canonical(ob, oo)
+    # Node bounds are the same floats, node by node of the canonical trees.
+    assert sorted(map(tuple, gb.bounds.reshape(-1, 6).tolist())) == sorted(map(tuple, ob.bounds.reshape(-1, 6).tolist()))
+
+
+def test_gpu_bvh_small_scene_matches_oracle(gpu):
+    b = scenes.small_scene()
+    shading, meshes = compile_shading(b.scene)
+    ids = {id(m): i for i, m in enumerate(shading.material_objects)}
+    sink = flatten_meshes(meshes, lambda m: ids.get(id(m), 0))
+    o = cpu.compile_sink(sink)
+    g = gpu.compile_sink(sink)
+    assert g.bvh.node_count == o.bvh.node_count
+    assert leaf_sets(g.bvh, g.order) == leaf_sets(o.bvh, o.order)
+    # Per-triangle data is identical once both are mapped back to input order.
+    inv_o = np.argsort(o.order)
+    inv_g = np.argsort(g.order)
+    for name, width in (("triangles", 9), ("normals", 9), ("uvs", 6), ("tangents", 4)):
+        a = getattr(o, name).reshape(-1, width)[inv_o]
+        c = getattr(g, name).reshape(-1, width)[inv_g]
+        assert np.array_equal(a, c), name
+    for name in ("materials", "flags", "sides"):
+        assert np.array_equal(getattr(o, name)[inv_o], getattr(g, name)[inv_g]), name
+    assert g.epsilon == o.epsilon
+
+
+def test_gpu_bvh_coincident_and_empty(gpu):
+    same = np.tile(np.array([0, 0, 0, 1, 0, 0, 0, 1, 0], np.float32), 500)
+    gb, go = gpu.build_bvh(same, 500)
+    assert gb.node_count > 1 and sorted(go.tolist()) == list(range(500))
+    # Every leaf respects the depth limit, and leaves cover every triangle once.
+    assert sum(len(s) for s in leaf_sets(gb, go)) == 500
+    eb, eo = gpu.build_bvh(np.zeros(0, np.float32), 0)
+    assert eb.node_count == 0
+
+
+# -------------------------------------------------------------- closest hits
+def _upload_triangles(gpu, raw, count, sides_value=2):
+    from meercadraytracer_b200.types import CompiledGeometry
+
+    bvh, order = cpu.build_bvh(raw, count)
+    data = reorder(raw, order)
+    g = CompiledGeometry(count, data, np.zeros(count * 9, np.float32), np.zeros(count * 6, np.float32),
+                         np.zeros(count * 4, np.float32), np.zeros(0, np.float32), np.zeros(count, np.uint32),
+                         np.ones(count, np.uint8), np.full(count, sides_value, np.uint8), bvh, 1e-4, order)
+    gpu._versions += 1
+    v = gpu._versions
+    gpu.send({"type": "geometry", "version": v, "geometry": g})
+    return v, data, bvh
+
+
+def test_gpu_closest_and_any_match_brute_force(gpu):  # bvh.test.ts:82-107 on the GPU
+    raw = lcg_triangles(3000, 7)
+    v, data, bvh = _upload_triangles(gpu, raw, 3000)
+    rays = np.zeros((400, 8), np.float32)
+    for i in range(400):
+        o, d = lissajous_ray(i)
+        rays[i, 0:3] = o
+        rays[i, 4:7] = d
+    hits = gpu.intersect_closest(v, rays, cull=True)
+    counts = gpu.intersect_any_count(v, rays)
+    found = 0
+    bad = []
+    for i in range(400):
+        # Brute force on the float32 ray the GPU was given.
+        o, d = rays[i, 0:3].astype(np.float64), rays[i, 4:7].astype(np.float64)
+        best, tri, allhits = brute_force(data, o, d)
+        ok = (hits["tri"][i] >= 0) == (tri >= 0) and counts[i] == allhits
+        if tri >= 0:
+            found += 1
+            ok = ok and hits["tri"][i] == tri and abs(hits["t"][i] - best) <= 1e-5 * best
+        if not ok:
+            bad.append((i, list(o), list(d), int(hits["tri"][i]), float(hits["t"][i]), tri, best, int(counts[i]),
+                        allhits))
+    assert not bad, bad[:5]
+    assert found > 100
+
+
+def test_gpu_culling_and_flat_box(gpu):  # bvh.test.ts:109-133
+    tri = np.array([-1, -1, 0, 2, 0, 0, 0, 2, 0], np.float32)
+    for side, front_hit, back_hit in ((0, True, False), (1, False, True), (2, True, True)):
+        v, _, _ = _upload_triangles(gpu, tri, 1, side)
+        rays = np.array([[0, 0, 5, 0, 0, 0, -1, 0], [0, 0, -5, 0, 0, 0, 1, 0]], np.float32)
+        h = gpu.intersect_closest(v, rays, cull=True)
+        assert (h["tri"][0] >= 0) == front_hit and (h["tri"][1] >= 0) == back_hit
+        if front_hit:
+            assert h["front"][0] == 1
+        if back_hit:
+            assert h["front"][1] == 0
+    quad = np.array([-1, -1, 0, 2, 0, 0, 2, 2, 0, -1, -1, 0, 2, 2, 0, 0, 2, 0], np.float32)
+    v, _, _ = _upload_triangles(gpu, quad, 2)
+    h = gpu.intersect_closest(v, np.array([[-1, 0, 3, 0, 0, 0, -1, 0]], np.float32))
+    assert h["tri"][0] >= 0 and abs(h["t"][0] - 3) < 1e-6
+
+
+# ----------------------------------------------------------- scene parity
+@pytest.fixture(scope="module")
+def small():
+    b = scenes.small_scene()
+    compiled = compile_scene(b.scene, builder=cpu.compile_sink)
+    return b, compiled, compile_camera(b.camera)
+
+
+def _all_pixels(w, h):
+    ys, xs = np.mgrid[0:h, 0:w]
+    return xs.ravel().astype(np.int32), ys.ravel().astype(np.int32)
+
+
+@pytest.mark.parametrize("pass_", [0, 3])
+def test_gpu_primary_hits_small_scene(gpu, small, pass_):
+    b, compiled, cam = small
+    px, py = _all_pixels(b.width, b.height)
+    o = cpu.trace_primary(compiled, cam, b.width, b.height, pass_, 0, px, py, threads=8)
+    g = gpu.trace_primary(compiled, cam, b.width, b.height, pass_, 0, px, py)
+    same = g["tri"] == o["tri"]
+    agree = same.mean()
+    hit = o["tri"] >= 0
+    # Disagreements must be ties: both hit at the same distance (a shared edge).
+    diff = ~same
+    ties = diff & (g["tri"] >= 0) & hit & (np.abs(g["t"] - o["t"]) <= 1e-5 * np.abs(o["t"]))
+    assert agree >= 0.9999 or (diff == ties).all(), (agree, int(diff.sum()), int(ties.sum()))
+    rel = np.abs(g["t"][hit & same] - o["t"][hit & same]) / o["t"][hit & same]
+    assert rel.max() <= 1e-5, rel.max()
+
+
+def _within_one_level(a, b):
+    d = np.abs(a.astype(np.int32) - b.astype(np.int32)).reshape(-1, 4)
+    return (d <= 1).all(axis=1).mean(), d.max()
+
+
+def test_gpu_small_scene_render_matches_oracle(gpu, small):
+    b, compiled, cam = small
+    o = as_options(b.options)
+    st, n, srgb = trace_settings(o), sample_count(o), output_srgb(o)
+    ref = cpu.raytrace_compiled(compiled, cam, b.width, b.height, st, n, srgb, threads=8)
+    out = gpu.raytrace(compiled, cam, b.width, b.height, st, n, srgb)
+    frac, worst = _within_one_level(out, ref)
+    assert frac >= 0.999, (frac, worst)
+
+
+def test_gpu_render_is_deterministic(gpu, small):
+    b, compiled, cam = small
+    o = as_options(b.options)
+    st = trace_settings(o)
+    a = gpu.raytrace(compiled, cam, b.width, b.height, st, 4, True)
+    c = gpu.raytrace(compiled, cam, b.width, b.height, st, 4, True)
+    assert np.array_equal(a, c)
+
+
+def test_gpu_render_pixels_match_full_render(gpu, small):
+    b, compiled, cam = small
+    st = trace_settings(as_options(b.options))
+    full = gpu.raytrace(compiled, cam, b.width, b.height, st, 5, True).reshape(-1, 4)
+    rng = np.random.default_rng(5)
+    idx = rng.choice(b.width * b.height, 500, replace=False)
+    px, py = (idx % b.width).astype(np.int32), (idx // b.width).astype(np.int32)
+    rgba, _ = gpu.render_pixels(compiled, cam, b.width, b.height, st, 5, True, px, py)
+    assert np.array_equal(rgba, full[idx])
+
+
+@pytest.mark.parametrize("block", [1, 4])
+def test_gpu_render_tile_matches_oracle(gpu, small, block):
+    from meercadraytracer_b200.types import Tile
+
+    b, compiled, cam = small
+    st = trace_settings(as_options(b.options))
+    tile = Tile(96, 64, 64, 48)
+    ref = cpu.render_tile(compiled, cam, st, tile, b.width, b.height, 2, block).reshape(-1, 4)
+    gpu.load_scene(compiled)
+    gv, sv = gpu._slots
+    fut = gpu.render({"type": "tile", "job": 1, "geometry_version": gv, "shading_version": sv, "camera": cam,
+                      "settings": st, "tile": tile, "width": b.width, "height": b.height, "pass": 2, "block": block})
+    out = fut.result().reshape(-1, 4)
+    close = (np.abs(out - ref) <= 2e-3 + 2e-3 * np.abs(ref)).all(axis=1)
+    assert close.mean() >= 0.999, close.mean()
+
+
+def test_gpu_tile_for_unknown_scene_is_an_error(gpu, small):
+    from meercadraytracer_b200.types import Tile
+
+    b, compiled, cam = small
+    gpu.load_scene(compiled)
+    fut = gpu.render({"type": "tile", "job": 1, "geometry_version": 987654, "shading_version": 1, "camera": cam,
+                      "settings": trace_settings({}), "tile": Tile(0, 0, 4, 4), "width": 8, "height": 8,
+                      "pass": 0, "block": 1})
+    with pytest.raises(McrtError) as err:
+        fut.result()
+    assert err.value.code == 3
+    assert "has not received" in str(err.value)
+
+
+def test_gpu_rejects_malformed_bvh(gpu):
+    from meercadraytracer_b200.types import CompiledBvh, CompiledGeometry
+
+    n = 2
+    bad = CompiledBvh(np.zeros(18, np.float32), np.array([1, 0, 0, 0, 2, 0, 5, 9, 0], np.int32), 3)
+    g = CompiledGeometry(n, np.zeros(18, np.float32), np.zeros(18, np.float32), np.zeros(12, np.float32),
+                         np.zeros(8, np.float32), np.zeros(0, np.float32), np.zeros(n, np.uint32),
+                         np.ones(n, np.uint8), np.zeros(n, np.uint8), bad, 1e-4)
+    with pytest.raises(McrtError) as err:
+        gpu.send({"type": "geometry", "version": 5, "geometry": g})
+    assert err.value.code == 1
