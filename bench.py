@@ -56,14 +56,24 @@ def measured_peaks() -> Dict[str, Any]:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def load_config(name: str):
+def load_config(name: str, width: int = 0, height: int = 0, spp: int = 0):
+    """The benchmark scene; width / height / spp override its image (for profiling runs)."""
     from meercadraytracer_b200 import scenes
 
     if name == "small":
-        return scenes.small_scene()
-    if name == "mid":
-        return scenes.mid_scene()
-    raise SystemExit(f"unknown config {name}")
+        b = scenes.small_scene()
+    elif name == "mid":
+        b = scenes.mid_scene()
+    else:
+        raise SystemExit(f"unknown config {name}")
+    if width or height or spp:
+        b.width = width or b.width
+        b.height = height or b.height
+        b.options = dict(b.options, samples=spp or b.options["samples"])
+        if hasattr(b.camera, "aspect"):
+            b.camera.aspect = b.width / b.height
+        b.name += f" (resized to {b.width}x{b.height}, {b.options['samples']} spp)"
+    return b
 
 
 class ClockSampler:
@@ -162,7 +172,7 @@ def run_reference(args, rank: int) -> None:
     from meercadraytracer_b200.compile import compile_camera, compile_scene
     from oracle import cpu
 
-    bench = load_config(args.config)
+    bench = load_config(args.config, args.width, args.height, args.spp)
     compiled = compile_scene(bench.scene, builder=cpu.compile_sink)
     cam = compile_camera(bench.camera)
     threads = os.cpu_count() or 1
@@ -206,7 +216,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = dist_mod
 
-    bench = load_config(args.config)
+    bench = load_config(args.config, args.width, args.height, args.spp)
     o = as_options(bench.options)
     st, spp, srgb = trace_settings(o), sample_count(o), output_srgb(o)
     ex = GpuExecutor(local)
@@ -265,29 +275,36 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     value = all_rays / (device_ms / 1000.0) / 1e6
     launches = int(s["launches"])
 
-    # End to end through the public API: host image read back every step.
-    ex.reset_stats()
-    e2e_times = []
-    for _ in range(args.steps):
-        flush.fill_(1)
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        res = raytrace_compiled(compiled, cam, w, h, o, executor=ex)
-        e2e_times.append(time.perf_counter() - t1)
-    e2e_rays = ex.stats()
-    e2e_value = (e2e_rays["closest_rays"] + e2e_rays["any_rays"]) / sum(e2e_times) / 1e6 * world
-    h2d = C.sizeof(abi.mcrt_camera) + C.sizeof(abi.mcrt_settings)
-    d2h = int(res.data.nbytes)
-
-    # Kernel breakdown of one frame (events around every kernel) for the roofline.
-    ex.reset_stats()
-    ex.set_timing(True)
-    frame()
-    ex.set_timing(False)
-    k = ex.stats()
-    kernels = {name: {"ms": k[f"ms_{name}"], "launches": k[f"n_{name}"]}
-               for name in ("raygen", "extend", "shade", "shadow", "resolve", "accumulate")}
-    top = max(("extend", "shadow"), key=lambda n: kernels[n]["ms"])
+    e2e = None
+    kernels = None
+    top = "extend"
+    k: Dict[str, Any] = {}
+    if not args.no_e2e:
+        # End to end through the public API: host image read back every step.
+        ex.reset_stats()
+        e2e_times = []
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            res = raytrace_compiled(compiled, cam, w, h, o, executor=ex)
+            e2e_times.append(time.perf_counter() - t1)
+        e2e_rays = ex.stats()
+        e2e_value = (e2e_rays["closest_rays"] + e2e_rays["any_rays"]) / sum(e2e_times) / 1e6 * world
+        e2e = {"value": round(e2e_value, 3), "unit": UNIT,
+               "h2d_bytes_per_step": C.sizeof(abi.mcrt_camera) + C.sizeof(abi.mcrt_settings),
+               "d2h_bytes_per_step": int(res.data.nbytes),
+               "note": "scene resident in HBM (uploaded once per geometry/shading version, as the executor "
+                       "protocol ships it); per step the camera and settings go down and the RGBA8 image comes back"}
+        # Kernel breakdown of one frame (events around every kernel) for the roofline.
+        ex.reset_stats()
+        ex.set_timing(True)
+        frame()
+        ex.set_timing(False)
+        k = ex.stats()
+        kernels = {name: {"ms": k[f"ms_{name}"], "launches": k[f"n_{name}"]}
+                   for name in ("raygen", "extend", "shade", "shadow", "resolve", "accumulate")}
+        top = max(("extend", "shadow"), key=lambda n: kernels[n]["ms"])
 
     if dist:
         dist.barrier()
@@ -304,19 +321,17 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         "data": "synthetic (seeded scene, no dataset)",
         "config": {"workload": bench.name, "triangles": bench.triangles, "width": w, "height": h, "spp": spp,
                    "rays_per_step": rays / args.steps, "l2": "flushed between steps (512 MiB write)",
-                   "parallelism": "replicas" if world > 1 else "single GPU", "path_capacity": ex.stats()["path_bytes"],
+                   "parallelism": "replicas" if world > 1 else "single GPU", "path_state_bytes": ex.stats()["path_bytes"],
                    "compile_s": {"flatten_host": round(t_flat, 3), "gpu_bvh_compile": round(t_build, 3),
                                  "upload": round(t_upload, 3)}},
         "wall_s_timed": round(wall, 3),
         "gpu_launches": launches,
         "clocks": clk,
-        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "note": "scene resident in HBM (uploaded once per geometry/shading version, as the executor "
-                        "protocol ships it); per step the camera and settings go down and the RGBA8 image comes back"},
+        "e2e": e2e,
         "kernels": kernels,
     }
     peaks = measured_peaks()
-    if world == 1 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline and kernels is not None:
         from oracle import cpu
 
         threads = os.cpu_count() or 1
@@ -365,6 +380,10 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="length of the CPU baseline sample")
     ap.add_argument("--ref-seconds", type=float, default=10.0, help="length of each reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and kernel-breakdown passes")
+    ap.add_argument("--width", type=int, default=0, help="override the image width (profiling runs)")
+    ap.add_argument("--height", type=int, default=0, help="override the image height (profiling runs)")
+    ap.add_argument("--spp", type=int, default=0, help="override samples per pixel (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be at least 3")

@@ -23,6 +23,7 @@
 #include "mcrt.h"
 #include "render.cuh"
 #include "scene_build.cuh"
+#include "traverse.cuh"
 
 namespace mcrt {
 namespace {
@@ -107,9 +108,21 @@ __global__ void k_pack_nodes(const float* __restrict__ bounds, const int* __rest
   d.lxy = make_float4(bl[0], bl[3], bl[1], bl[4]);
   d.rxy = make_float4(br[0], br[3], br[1], br[4]);
   d.lrz = make_float4(bl[2], bl[5], br[2], br[5]);
+  // Child references: an inner node's index, or ~first for a leaf.
   const int lc = nodes[3 * l + 1], rc = nodes[3 * r + 1];
-  d.kids = make_int4(lc > 0 ? nodes[3 * l] : index[l], rc > 0 ? nodes[3 * r] : index[r], lc, rc);
+  d.kids = make_int4(lc > 0 ? ~nodes[3 * l] : index[l], rc > 0 ? ~nodes[3 * r] : index[r], lc, rc);
   out[index[i]] = d;
+}
+
+// Flags the last triangle of every leaf (kLeafEnd), which ends the leaf's
+// triangle loop during traversal.
+__global__ void k_mark_leaf_ends(const int* __restrict__ nodes, int m, float4* __restrict__ tris) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int first = nodes[3 * i], count = nodes[3 * i + 1];
+  if (count <= 0) return;
+  float4* t = tris + 3 * static_cast<size_t>(first + count - 1);
+  t->w = __int_as_float(__float_as_int(t->w) | kLeafEnd);
 }
 
 int blocks(long long n, int b) { return static_cast<int>((n + b - 1) / b); }
@@ -186,7 +199,7 @@ struct mcrt_executor {
   ShadingGpu sh;
   std::unordered_map<int, std::unique_ptr<TextureGpu>> textures;
   PathBuffers paths;
-  int capacity = 1 << 22;
+  int capacity = 1 << 24;  // paths in flight: 16M, about 9 GB of path state with 5 lights
   bool timed = false;
   RenderStats stats;
   double ms_total = 0;
@@ -476,10 +489,12 @@ int32_t mcrt_send_geometry(mcrt_executor* ex, int32_t version, const mcrt_geomet
       G.tangents.upload(g->tangents, sizeof(float) * 4 * n, s);
       G.has_colors = g->colors != nullptr;
       if (G.has_colors) G.colors.upload(g->colors, sizeof(float) * 12 * n, s);
+      DevBuf nodes;
+      nodes.upload(g->bvh_nodes, sizeof(int) * 3 * m, s);
+      k_mark_leaf_ends<<<blocks(m, 256), 256, 0, s>>>(nodes.as<int>(), m, G.tris.as<float4>());
       if (G.root_count == 0) {
-        DevBuf bounds, nodes, flag, index, temp;
+        DevBuf bounds, flag, index, temp;
         bounds.upload(g->bvh_bounds, sizeof(float) * 6 * m, s);
-        nodes.upload(g->bvh_nodes, sizeof(int) * 3 * m, s);
         flag.ensure(sizeof(int) * m);
         index.ensure(sizeof(int) * m);
         k_inner_flags<<<blocks(m, 256), 256, 0, s>>>(nodes.as<int>(), m, flag.as<int>());
@@ -812,7 +827,12 @@ int32_t mcrt_intersect_closest(mcrt_executor* ex, int32_t gv, int32_t count, con
     if (count == 0) return;
     float4* r = static_cast<float4*>(ex->rays.upload(rays, sizeof(float) * 8 * count, ex->stream));
     int4* h = static_cast<int4*>(ex->hits.ensure(sizeof(int4) * count));
-    cuda_check(launch_trace_rays(make_scene(ex), r, count, cull, h, ex->stream), "trace");
+    unsigned* fetch = static_cast<unsigned*>(ex->scratch.ensure(2 * sizeof(unsigned)));
+    cuda_check(cudaMemsetAsync(fetch + 1, 0, sizeof(unsigned), ex->stream), "memset");
+    cuda_check(launch_trace_rays(make_scene(ex), r, count, cull, h, fetch, ex->stream), "trace");
+    unsigned walk_status = 0;
+    download(ex, &walk_status, fetch + 1, sizeof(unsigned), "download");
+    ex->stats.status |= walk_status;
     std::vector<int4> out(count);
     download(ex, out.data(), h, sizeof(int4) * count, "download");
     for (int i = 0; i < count; i++) {
@@ -832,7 +852,8 @@ int32_t mcrt_intersect_any_count(mcrt_executor* ex, int32_t gv, int32_t count, c
     if (count == 0) return;
     float4* r = static_cast<float4*>(ex->rays.upload(rays, sizeof(float) * 8 * count, ex->stream));
     int* c = static_cast<int*>(ex->hits.ensure(sizeof(int) * count));
-    cuda_check(launch_count_hits(make_scene(ex), r, count, c, ex->stream), "trace");
+    unsigned* fetch = static_cast<unsigned*>(ex->scratch.ensure(sizeof(unsigned)));
+    cuda_check(launch_count_hits(make_scene(ex), r, count, c, fetch, ex->stream), "trace");
     download(ex, counts, c, sizeof(int) * count, "download");
   });
 }

@@ -115,22 +115,39 @@ __global__ void __launch_bounds__(kBlock) k_raygen(FrameParams fp, PathState ps,
 }
 
 // ------------------------------------------------------------------ extend
+// Closest hit of each queued path's ray (intersectClosest, bvh.ts:202-282),
+// persistent: warps take rays from cnt->fetch until the queue is drained.
+struct ExtendQuery {
+  const DScene& sc;
+  const PathState& ps;
+  const int* queue;
+  int pid;
+  ClosestState cs;
+  MCRT_D void load(int i) {
+    pid = queue[i];
+    const float4 o = ps.ray_o[pid], d = ps.ray_d[pid];
+    cs.start(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, (ps.flags[pid] & kFlagCull) != 0);
+  }
+  MCRT_D const TravRay& ray() const { return cs.r; }
+  MCRT_D float t_max() const { return cs.tmax; }
+  MCRT_D bool leaf(int first) { return cs.leaf(sc, first); }
+  MCRT_D void finish() {
+    const ClosestHit& h = cs.h;
+    const unsigned word = h.tri >= 0 ? ((h.front ? 0x80000000u : 0u) | static_cast<unsigned>(h.tri + 1)) : 0u;
+    ps.hit[pid] = make_float4(h.t, h.u, h.v, __uint_as_float(word));
+  }
+};
+
 __global__ void __launch_bounds__(kBlock) k_extend(DScene sc, PathState ps, const int* __restrict__ queue, int n,
                                                    Counters* cnt) {
   __shared__ int stack_mem[kShort * kBlock];
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n) return;
-  const int pid = queue[q];
-  const float4 o = ps.ray_o[pid], d = ps.ray_d[pid];
-  const bool cull = (ps.flags[pid] & kFlagCull) != 0;
   TravStack st;
   st.smem = stack_mem + threadIdx.x;
   st.stride = kBlock;
+  st.sp = 0;
   unsigned status = 0;
-  TravRay r = make_trav_ray(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z});
-  ClosestHit h = trace_closest(sc, r, cull, st, status);
-  unsigned word = h.tri >= 0 ? ((h.front ? 0x80000000u : 0u) | static_cast<unsigned>(h.tri + 1)) : 0u;
-  ps.hit[pid] = make_float4(h.t, h.u, h.v, __uint_as_float(word));
+  ExtendQuery q{sc, ps, queue, 0, {}};
+  traverse_persistent(sc, q, n, &cnt->fetch, st, status);
   if (status) atomicOr(&cnt->status, status);
 }
 
@@ -630,90 +647,118 @@ __global__ void __launch_bounds__(kBlock) k_shade(DScene sc, FrameParams fp, Pat
 }
 
 // ------------------------------------------------------------------ shadow
-// transmittance / attenuateShadow, tracer.ts:529-594, for one shadow ray.
-__global__ void __launch_bounds__(kBlock) k_shadow(DScene sc, PathState ps, int n, int capacity, Counters* cnt) {
-  __shared__ int stack_mem[kShort * kBlock];
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const float4* e = ps.shadow_queue + 3 * static_cast<size_t>(s);
-  const float4 e0 = e[0], e1 = e[1], e2 = e[2];
-  const int pid = __float_as_int(e1.w);
-  const int tag = __float_as_int(e2.w);
-  const int slot = tag & 0xffff;
-  const bool cast_only = (tag & 0x10000) != 0;
-  const float max_t = e0.w;
-  TravStack st;
-  st.smem = stack_mem + threadIdx.x;
-  st.stride = kBlock;
-  unsigned status = 0;
-  TravRay r = make_trav_ray(V3{e0.x, e0.y, e0.z}, V3{e1.x, e1.y, e1.z});
-  V3 shadow = V3{1.0f, 1.0f, 1.0f};
-  V3 depth = V3{0.0f, 0.0f, 0.0f};
+// transmittance / attenuateShadow, tracer.ts:529-594, for one shadow ray: the
+// any-hit walk stops at an opaque triangle or when almost no light is left.
+struct ShadowQuery {
+  const DScene& sc;
+  const PathState& ps;
+  int capacity;
+  unsigned* status;
+  int pid, slot;
+  bool cast_only, blocked;
+  float max_t;
+  TravRay r;
+  V3 w, shadow, depth;
+  int nseen;
   float seen[kShadowSeen];
-  int nseen = 0;
-  bool blocked = false;
-  float tm = max_t;
-  traverse(sc, r, tm, st, status, [&](int first, int count, float&) {
-    for (int k = first; k < first + count; k++) {
+  MCRT_D void load(int i) {
+    const float4* e = ps.shadow_queue + 3 * static_cast<size_t>(i);
+    const float4 e0 = e[0], e1 = e[1], e2 = e[2];
+    pid = __float_as_int(e1.w);
+    const int tag = __float_as_int(e2.w);
+    slot = tag & 0xffff;
+    cast_only = (tag & 0x10000) != 0;
+    max_t = e0.w;
+    r = make_trav_ray(V3{e0.x, e0.y, e0.z}, V3{e1.x, e1.y, e1.z});
+    w = V3{e2.x, e2.y, e2.z};
+    shadow = V3{1.0f, 1.0f, 1.0f};
+    depth = V3{0.0f, 0.0f, 0.0f};
+    nseen = 0;
+    blocked = false;
+  }
+  MCRT_D const TravRay& ray() const { return r; }
+  MCRT_D float t_max() const { return max_t; }
+  MCRT_D bool leaf(int first) {
+    for (int k = first; k < sc.tri_count; k++) {
       V3 a, b, c;
       float4 w0, w1;
       load_tri(sc, k, a, b, c, w0, w1);
+      const bool last = leaf_end(w0.w);
       TriHit th;
-      if (!intersect_triangle(r, a, b, c, max_t, 2, th)) continue;
-      const int fl = tri_flags(w0.w);
-      if (cast_only && (fl & 2) == 0) continue;
-      if (fl & 1) {
-        blocked = true;
-        return false;
-      }
-      const DMaterial& mat = sc.materials[__float_as_int(w1.w)];
-      float alpha = mat.opacity;
-      V3 col = V3{mat.color[0], mat.color[1], mat.color[2]};
-      if (mat.map >= 0 || mat.alpha_map >= 0) {
-        const float4* at = sc.attrs + 4 * static_cast<size_t>(k);
-        const float4 a2 = __ldg(at + 2), a3 = __ldg(at + 3);
-        const float ww0 = 1.0f - th.u - th.v;
-        const float tu = a2.y * ww0 + a2.w * th.u + a3.y * th.v;
-        const float tv = a2.z * ww0 + a3.x * th.u + a3.z * th.v;
-        if (mat.map >= 0) {
-          const float4 tx = sample_texture(sc, mat.map, tu, tv);
-          alpha *= tx.w;
-          col = col * V3{tx.x, tx.y, tx.z};
-        }
-        if (mat.alpha_map >= 0) alpha *= sample_texture(sc, mat.alpha_map, tu, tv).y;
-      }
-      if (mat.alpha_test > 0.0f && alpha < mat.alpha_test) continue;
-      if (!mat.transparent) alpha = 1.0f;
-      bool dup = false;
-      for (int i = 0; i < nseen; i++) dup |= fabsf(seen[i] - th.t) <= sc.eps;
-      if (dup) continue;
-      if (nseen < kShadowSeen) {
-        seen[nseen++] = th.t;
-      } else {
-        status |= kStatusShadowListOverflow;
-      }
-      if (mat.thickness > 0.0f) {
-        const float sgn = th.front ? -th.t : th.t;
-        depth = depth + V3{mat.attenuation[0], mat.attenuation[1], mat.attenuation[2]} * sgn;
-      }
-      const float open = 1.0f - alpha;
-      const float through = mat.transmission;
-      shadow = shadow * (V3{open, open, open} + col * (alpha * through));
-      if (shadow.x + shadow.y + shadow.z < 1e-4f) {
-        blocked = true;
-        return false;
-      }
+      if (intersect_triangle(r, a, b, c, max_t, 2, th) && visit(k, th, w0, w1)) return false;
+      if (last) break;
     }
     return true;
-  });
-  V3 result = V3{0.0f, 0.0f, 0.0f};
-  if (!blocked) {
-    if (depth.x > 0.0f) shadow.x *= expf(-depth.x);
-    if (depth.y > 0.0f) shadow.y *= expf(-depth.y);
-    if (depth.z > 0.0f) shadow.z *= expf(-depth.z);
-    if (shadow.x + shadow.y + shadow.z > 0.0f) result = V3{e2.x, e2.y, e2.z} * shadow;
   }
-  ps.slots[static_cast<size_t>(slot) * capacity + pid] = make_float4(result.x, result.y, result.z, 0.0f);
+  // One hit of the visitor; true once the ray is blocked.
+  MCRT_D bool visit(int k, const TriHit& th, float4 w0, float4 w1) {
+    const int fl = tri_flags(w0.w);
+    if (cast_only && (fl & 2) == 0) return false;
+    if (fl & 1) {
+      blocked = true;
+      return true;
+    }
+    const DMaterial& mat = sc.materials[__float_as_int(w1.w)];
+    float alpha = mat.opacity;
+    V3 col = V3{mat.color[0], mat.color[1], mat.color[2]};
+    if (mat.map >= 0 || mat.alpha_map >= 0) {
+      const float4* at = sc.attrs + 4 * static_cast<size_t>(k);
+      const float4 a2 = __ldg(at + 2), a3 = __ldg(at + 3);
+      const float ww0 = 1.0f - th.u - th.v;
+      const float tu = a2.y * ww0 + a2.w * th.u + a3.y * th.v;
+      const float tv = a2.z * ww0 + a3.x * th.u + a3.z * th.v;
+      if (mat.map >= 0) {
+        const float4 tx = sample_texture(sc, mat.map, tu, tv);
+        alpha *= tx.w;
+        col = col * V3{tx.x, tx.y, tx.z};
+      }
+      if (mat.alpha_map >= 0) alpha *= sample_texture(sc, mat.alpha_map, tu, tv).y;
+    }
+    if (mat.alpha_test > 0.0f && alpha < mat.alpha_test) return false;
+    if (!mat.transparent) alpha = 1.0f;
+    bool dup = false;
+    for (int i = 0; i < nseen; i++) dup |= fabsf(seen[i] - th.t) <= sc.eps;
+    if (dup) return false;
+    if (nseen < kShadowSeen) {
+      seen[nseen++] = th.t;
+    } else {
+      *status |= kStatusShadowListOverflow;
+    }
+    if (mat.thickness > 0.0f) {
+      const float sgn = th.front ? -th.t : th.t;
+      depth = depth + V3{mat.attenuation[0], mat.attenuation[1], mat.attenuation[2]} * sgn;
+    }
+    const float open = 1.0f - alpha;
+    const float through = mat.transmission;
+    shadow = shadow * (V3{open, open, open} + col * (alpha * through));
+    if (shadow.x + shadow.y + shadow.z < 1e-4f) {
+      blocked = true;
+      return true;
+    }
+    return false;
+  }
+  MCRT_D void finish() {
+    V3 result = V3{0.0f, 0.0f, 0.0f};
+    if (!blocked) {
+      V3 s = shadow;
+      if (depth.x > 0.0f) s.x *= expf(-depth.x);
+      if (depth.y > 0.0f) s.y *= expf(-depth.y);
+      if (depth.z > 0.0f) s.z *= expf(-depth.z);
+      if (s.x + s.y + s.z > 0.0f) result = w * s;
+    }
+    ps.slots[static_cast<size_t>(slot) * capacity + pid] = make_float4(result.x, result.y, result.z, 0.0f);
+  }
+};
+
+__global__ void __launch_bounds__(kBlock) k_shadow(DScene sc, PathState ps, int n, int capacity, Counters* cnt) {
+  __shared__ int stack_mem[kShort * kBlock];
+  TravStack st;
+  st.smem = stack_mem + threadIdx.x;
+  st.stride = kBlock;
+  st.sp = 0;
+  unsigned status = 0;
+  ShadowQuery q{sc, ps, capacity, &status};
+  traverse_persistent(sc, q, n, &cnt->fetch, st, status);
   if (status) atomicOr(&cnt->status, status);
 }
 
@@ -814,48 +859,81 @@ __global__ void k_tile_output(const float4* __restrict__ samples, FrameParams fp
 }
 
 // Closest hits of arbitrary rays (origin, -, direction, -): debugging and parity.
+struct RayQuery {
+  const DScene& sc;
+  const float4* rays;
+  int cull;
+  int4* hits;
+  int i;
+  ClosestState cs;
+  MCRT_D void load(int k) {
+    i = k;
+    const float4 o = rays[2 * k], d = rays[2 * k + 1];
+    cs.start(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, cull != 0);
+  }
+  MCRT_D const TravRay& ray() const { return cs.r; }
+  MCRT_D float t_max() const { return cs.tmax; }
+  MCRT_D bool leaf(int first) { return cs.leaf(sc, first); }
+  MCRT_D void finish() {
+    hits[i] = make_int4(cs.h.tri, __float_as_int(cs.h.t), __float_as_int(cs.h.u),
+                        (cs.h.front ? 1 : 0) | (min(cs.tests, 0xffffff) << 8));
+  }
+};
+
 __global__ void __launch_bounds__(kBlock) k_trace_rays(DScene sc, const float4* __restrict__ rays, int n, int cull,
-                                                       int4* __restrict__ hits) {
+                                                       int4* __restrict__ hits, unsigned* fetch) {
   __shared__ int stack_mem[kShort * kBlock];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float4 o = rays[2 * i], d = rays[2 * i + 1];
   TravStack st;
   st.smem = stack_mem + threadIdx.x;
   st.stride = kBlock;
+  st.sp = 0;
   unsigned status = 0;
-  TravRay r = make_trav_ray(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z});
-  ClosestHit h = trace_closest(sc, r, cull != 0, st, status);
-  hits[i] = make_int4(h.tri, __float_as_int(h.t), __float_as_int(h.u), (h.front ? 1 : 0) | (status << 8));
-  (void)h.v;
+  RayQuery q{sc, rays, cull, hits, 0, {}};
+  traverse_persistent(sc, q, n, fetch, st, status);
+  if (status) atomicOr(fetch + 1, status);
 }
 
 // Number of hits along each ray (intersectAny with a counting visitor).
-__global__ void __launch_bounds__(kBlock) k_count_hits(DScene sc, const float4* __restrict__ rays, int n,
-                                                       int* __restrict__ counts) {
-  __shared__ int stack_mem[kShort * kBlock];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float4 o = rays[2 * i], d = rays[2 * i + 1];
-  TravStack st;
-  st.smem = stack_mem + threadIdx.x;
-  st.stride = kBlock;
-  unsigned status = 0;
-  TravRay r = make_trav_ray(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z});
-  float tm = o.w > 0.0f ? o.w : __int_as_float(0x7f800000);
-  const float t_limit = tm;
-  int hits = 0;
-  traverse(sc, r, tm, st, status, [&](int first, int count, float&) {
-    for (int k = first; k < first + count; k++) {
+struct CountQuery {
+  const DScene& sc;
+  const float4* rays;
+  int* counts;
+  int i, hits;
+  float limit;
+  TravRay r;
+  MCRT_D void load(int k) {
+    i = k;
+    hits = 0;
+    const float4 o = rays[2 * k], d = rays[2 * k + 1];
+    limit = o.w > 0.0f ? o.w : __int_as_float(0x7f800000);
+    r = make_trav_ray(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z});
+  }
+  MCRT_D const TravRay& ray() const { return r; }
+  MCRT_D float t_max() const { return limit; }
+  MCRT_D bool leaf(int first) {
+    for (int k = first; k < sc.tri_count; k++) {
       V3 a, b, c;
       float4 w0, w1;
       load_tri(sc, k, a, b, c, w0, w1);
       TriHit th;
-      if (intersect_triangle(r, a, b, c, t_limit, 2, th)) hits++;
+      if (intersect_triangle(r, a, b, c, limit, 2, th)) hits++;
+      if (leaf_end(w0.w)) break;
     }
     return true;
-  });
-  counts[i] = hits;
+  }
+  MCRT_D void finish() { counts[i] = hits; }
+};
+
+__global__ void __launch_bounds__(kBlock) k_count_hits(DScene sc, const float4* __restrict__ rays, int n,
+                                                       int* __restrict__ counts, unsigned* fetch) {
+  __shared__ int stack_mem[kShort * kBlock];
+  TravStack st;
+  st.smem = stack_mem + threadIdx.x;
+  st.stride = kBlock;
+  st.sp = 0;
+  unsigned status = 0;
+  CountQuery q{sc, rays, counts, 0, 0, 0.0f, {}};
+  traverse_persistent(sc, q, n, fetch, st, status);
 }
 
 // ------------------------------------------------------------------- host
@@ -955,6 +1033,22 @@ struct Timer {
 
 inline int blocks_for(long long n, int block) { return static_cast<int>((n + block - 1) / block); }
 
+// Blocks of a persistent traversal launch: enough to fill every SM at the
+// kernel's occupancy, fewer when there is less work.
+template <class K>
+int persistent_blocks(K kernel, long long n) {
+  static int per_device[64][2] = {};  // cached (SMs, blocks per SM) per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int* c = per_device[dev & 63];
+  if (c[0] == 0) {
+    cudaDeviceGetAttribute(&c[0], cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c[1], kernel, kBlock, 0);
+    if (c[1] < 1) c[1] = 1;
+  }
+  return static_cast<int>(std::min<long long>(blocks_for(n, kBlock), static_cast<long long>(c[0]) * c[1]));
+}
+
 }  // namespace
 
 cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, PathBuffers& buffers,
@@ -993,8 +1087,9 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
         e = cudaErrorLaunchTimeout;
         break;
       }
+      cudaMemsetAsync(&cnt->fetch, 0, sizeof(unsigned int), stream);
       tm.start();
-      k_extend<<<blocks_for(n, kBlock), kBlock, 0, stream>>>(scene, ps, ps.queue[cur], n, cnt);
+      k_extend<<<persistent_blocks(k_extend, n), kBlock, 0, stream>>>(scene, ps, ps.queue[cur], n, cnt);
       tm.stop(st.ms_extend, st.n_extend);
       st.closest_rays += n;
       cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), stream);
@@ -1008,8 +1103,9 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
       const int n_shadow = static_cast<int>(host->shadow_count);
       st.status |= host->status;
       if (n_shadow > 0) {
+        cudaMemsetAsync(&cnt->fetch, 0, sizeof(unsigned int), stream);
         tm.start();
-        k_shadow<<<blocks_for(n_shadow, kBlock), kBlock, 0, stream>>>(scene, ps, n_shadow, cap, cnt);
+        k_shadow<<<persistent_blocks(k_shadow, n_shadow), kBlock, 0, stream>>>(scene, ps, n_shadow, cap, cnt);
         tm.stop(st.ms_shadow, st.n_shadow);
         st.any_rays += n_shadow;
         st.launches++;
@@ -1045,7 +1141,8 @@ cudaError_t primary_hits(const DScene& scene, FrameParams fp, PathBuffers& buffe
   fp.capacity = buffers.capacity();
   fp.slot_count = buffers.slots();
   k_raygen<<<blocks_for(n, kBlock), kBlock, 0, stream>>>(fp, ps, n);
-  k_extend<<<blocks_for(n, kBlock), kBlock, 0, stream>>>(scene, ps, ps.queue[0], n, buffers.counters());
+  cudaMemsetAsync(&buffers.counters()->fetch, 0, sizeof(unsigned int), stream);
+  k_extend<<<persistent_blocks(k_extend, n), kBlock, 0, stream>>>(scene, ps, ps.queue[0], n, buffers.counters());
   return cudaGetLastError();
 }
 
@@ -1063,15 +1160,18 @@ cudaError_t launch_tile_output(const float4* samples, const FrameParams& fp, flo
 }
 
 cudaError_t launch_trace_rays(const DScene& scene, const float4* rays, int count, int cull, int4* hits,
-                              cudaStream_t s) {
+                              unsigned* fetch, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
-  k_trace_rays<<<blocks_for(count, kBlock), kBlock, 0, s>>>(scene, rays, count, cull, hits);
+  cudaMemsetAsync(fetch, 0, sizeof(unsigned), s);
+  k_trace_rays<<<persistent_blocks(k_trace_rays, count), kBlock, 0, s>>>(scene, rays, count, cull, hits, fetch);
   return cudaGetLastError();
 }
 
-cudaError_t launch_count_hits(const DScene& scene, const float4* rays, int count, int* counts, cudaStream_t s) {
+cudaError_t launch_count_hits(const DScene& scene, const float4* rays, int count, int* counts, unsigned* fetch,
+                              cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
-  k_count_hits<<<blocks_for(count, kBlock), kBlock, 0, s>>>(scene, rays, count, counts);
+  cudaMemsetAsync(fetch, 0, sizeof(unsigned), s);
+  k_count_hits<<<persistent_blocks(k_count_hits, count), kBlock, 0, s>>>(scene, rays, count, counts, fetch);
   return cudaGetLastError();
 }
 

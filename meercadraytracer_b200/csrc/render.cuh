@@ -65,7 +65,7 @@ struct Counters {
   unsigned int next_count;
   unsigned int shadow_count;
   unsigned int status;
-  unsigned int pad;
+  unsigned int fetch;  // next query a persistent traversal warp takes
 };
 
 // Work and time of the kernels of one render, for benchmarks.
@@ -122,8 +122,10 @@ cudaError_t primary_hits(const DScene& scene, FrameParams fp, PathBuffers& buffe
 cudaError_t launch_accumulate(const float4* samples, int npix, int passes_in_chunk, float4* sum, int total_passes,
                               int last_chunk, uint8_t* image, const FrameParams& fp, int srgb, cudaStream_t s);
 cudaError_t launch_tile_output(const float4* samples, const FrameParams& fp, float* out, cudaStream_t s);
+// `fetch` is a device counter the persistent traversal uses (reset here).
 cudaError_t launch_trace_rays(const DScene& scene, const float4* rays, int count, int cull, int4* hits,
+                              unsigned* fetch, cudaStream_t s);
+cudaError_t launch_count_hits(const DScene& scene, const float4* rays, int count, int* counts, unsigned* fetch,
                               cudaStream_t s);
-cudaError_t launch_count_hits(const DScene& scene, const float4* rays, int count, int* counts, cudaStream_t s);
 
 }  // namespace mcrt

@@ -15,10 +15,20 @@
 // so rounding can't lose a box a ray grazes, which keeps flat boxes (planes)
 // hit as the reference's boxEntry does (src/bvh.ts:340-356).
 //
-// Traversal visits the nearer child first and pushes the other on a short
-// stack whose top kShort entries live in shared memory (one column per
-// thread, bank-conflict free) and whose rest spills to local memory; BVH depth
-// is at most kMaxDepth, so the stack is bounded.
+// The walk is the persistent "while-while" traversal of Aila and Laine
+// ("Understanding the Efficiency of Ray Traversal on GPUs", HPG 2009, and its
+// Kepler/Fermi follow-up): each lane descends inner nodes (nearer child
+// first, the other pushed) until every lane of the warp holds a leaf, then
+// the warp tests leaves together, which keeps SIMD lanes busy; when enough
+// lanes have finished their rays the warp refills them from a global counter
+// (dynamic fetch), so a warp never idles waiting on its slowest ray. The
+// stack keeps its top kShort entries in shared memory (one column per
+// thread, bank-conflict free) and spills to local memory; the builder bounds
+// depth at 100, and a deeper foreign tree sets a status bit instead of
+// overflowing.
+//
+// Child references: >= 0 an inner node index; < 0 a leaf whose first triangle
+// is ~ref. The last triangle of every leaf carries kLeafEnd in its flag word.
 #pragma once
 
 #include "device_scene.cuh"
@@ -26,10 +36,21 @@
 namespace mcrt {
 
 constexpr int kShort = 16;  // shared-memory stack entries per thread
+constexpr int kSentinel = 0x7fffffff;  // empty stack / finished ray
+constexpr int kLeafEnd = 1 << 16;      // in tris[3k].w: last triangle of its leaf
+constexpr int kRefill = 8;             // refill a warp's finished lanes once this many are idle
 
 // Status bits a kernel reports back (never a trap).
 constexpr unsigned kStatusStackOverflow = 1u;
 constexpr unsigned kStatusShadowListOverflow = 2u;
+constexpr unsigned kStatusStepLimit = 4u;  // a query hit the step budget and was ended
+constexpr unsigned kStatusLeafRange = 8u;  // a leaf ran past the last triangle and was cut
+
+// Node visits plus leaves one query may take: a walk of a well-formed BVH of
+// N triangles enters each of its fewer than 2N nodes at most once, so past
+// 2N + 64 steps something is wrong and the query ends (kStatusStepLimit)
+// instead of looping.
+MCRT_D int max_steps(const DScene& sc) { return 2 * sc.tri_count + 64; }
 
 struct TravRay {
   V3 o, d, inv;
@@ -114,14 +135,20 @@ MCRT_D float box_entry(const TravRay& r, float x0, float x1, float y0, float y1,
   return lo <= hi ? lo : -1.0f;
 }
 
-MCRT_D DNode load_node(const DNode* nodes, int i) {
+struct NodeRefs {
+  float4 lxy, rxy, lrz;
+  int left, right;
+};
+
+MCRT_D NodeRefs load_node(const DNode* nodes, int i) {
   const float4* p = reinterpret_cast<const float4*>(nodes + i);
-  DNode n;
+  NodeRefs n;
   n.lxy = __ldg(p);
   n.rxy = __ldg(p + 1);
   n.lrz = __ldg(p + 2);
-  float4 k = __ldg(p + 3);
-  n.kids = make_int4(__float_as_int(k.x), __float_as_int(k.y), __float_as_int(k.z), __float_as_int(k.w));
+  const float4 k = __ldg(p + 3);
+  n.left = __float_as_int(k.x);
+  n.right = __float_as_int(k.y);
   return n;
 }
 
@@ -142,62 +169,13 @@ struct TravStack {
     sp++;
     return true;
   }
+  // The top entry, or kSentinel when empty.
   MCRT_D int pop() {
+    if (sp == 0) return kSentinel;
     --sp;
     return sp < kShort ? smem[sp * stride] : spill[sp - kShort];
   }
 };
-
-// Walks the BVH, nearer child first, calling leaf(first, count, t_max) for
-// every leaf whose box the ray enters before t_max. `leaf` may lower t_max
-// (closest hit) and returns false to end the walk (any hit blocked).
-template <class Leaf>
-MCRT_D void traverse(const DScene& sc, const TravRay& r, float& t_max, TravStack& st, unsigned& status, Leaf&& leaf) {
-  if (sc.tri_count == 0) return;
-  if (sc.root_count > 0) {
-    leaf(0, sc.root_count, t_max);
-    return;
-  }
-  st.sp = 0;
-  int node = 0;
-  for (;;) {
-    const DNode n = load_node(sc.nodes, node);
-    float e0 = box_entry(r, n.lxy.x, n.lxy.y, n.lxy.z, n.lxy.w, n.lrz.x, n.lrz.y, t_max);
-    float e1 = box_entry(r, n.rxy.x, n.rxy.y, n.rxy.z, n.rxy.w, n.lrz.z, n.lrz.w, t_max);
-    int r0 = n.kids.x, c0 = n.kids.z, r1 = n.kids.y, c1 = n.kids.w;
-    bool h0 = e0 >= 0.0f && c0 >= 0;
-    bool h1 = e1 >= 0.0f && c1 >= 0;
-    if (h1 && (!h0 || e1 < e0)) {  // visit the nearer child first
-      int tr = r0; r0 = r1; r1 = tr;
-      int tc = c0; c0 = c1; c1 = tc;
-      float te = e0; e0 = e1; e1 = te;
-      bool th = h0; h0 = h1; h1 = th;
-    }
-    int next = -1;
-    if (h0) {
-      if (c0 > 0) {
-        if (!leaf(r0, c0, t_max)) return;
-      } else {
-        next = r0;
-      }
-    }
-    if (h1 && e1 <= t_max) {
-      if (c1 > 0) {
-        if (!leaf(r1, c1, t_max)) return;
-      } else if (next < 0) {
-        next = r1;
-      } else if (!st.push(r1)) {
-        status |= kStatusStackOverflow;
-      }
-    }
-    if (next >= 0) {
-      node = next;
-      continue;
-    }
-    if (st.sp == 0) return;
-    node = st.pop();
-  }
-}
 
 MCRT_D void load_tri(const DScene& sc, int k, V3& a, V3& b, V3& c, float4& w0, float4& w1) {
   const float4* p = sc.tris + 3 * static_cast<size_t>(k);
@@ -209,34 +187,160 @@ MCRT_D void load_tri(const DScene& sc, int k, V3& a, V3& b, V3& c, float4& w0, f
   c = V3{t2.x, t2.y, t2.z};
 }
 
+MCRT_D bool leaf_end(float w) { return (__float_as_int(w) & kLeafEnd) != 0; }
+
+MCRT_D unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Root reference of the scene: node 0, or the single leaf at triangle 0.
+MCRT_D int root_ref(const DScene& sc) { return sc.root_count > 0 ? ~0 : 0; }
+
+// Persistent while-while traversal of queries [0, n) for one warp, taking
+// work from *counter. Q supplies, per lane:
+//   void load(int index)      start query `index` (ray, limits, result state)
+//   const TravRay& ray()
+//   float t_max()             current upper limit (closest hit lowers it)
+//   bool leaf(int first)      test the leaf starting at triangle `first`;
+//                             false ends the query (any hit: blocked)
+//   void finish()             write the query's result
+template <class Q>
+MCRT_D void traverse_persistent(const DScene& sc, Q& q, int n, unsigned* counter, TravStack& st,
+                                unsigned& status) {
+  const unsigned lane = threadIdx.x & 31;
+  const bool empty = sc.tri_count == 0;
+  const int step_limit = max_steps(sc);
+  int node = kSentinel;  // next node to visit (kSentinel: none)
+  int leaf = 0;          // postponed leaf (< 0), or 0
+  int steps = 0;         // node visits and leaves of the current query
+  bool has = false;      // this lane holds an unfinished query
+  bool exhausted = false;
+  for (;;) {
+    // Refill finished lanes with one atomic per warp.
+    const bool need = !has && !exhausted;
+    const unsigned mneed = __ballot_sync(0xffffffffu, need);
+    if (mneed) {
+      const int leader = __ffs(mneed) - 1;
+      unsigned base = 0;
+      if (static_cast<int>(lane) == leader) base = atomicAdd(counter, __popc(mneed));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const unsigned idx = base + __popc(mneed & lanemask_lt());
+        if (idx < static_cast<unsigned>(n)) {
+          q.load(static_cast<int>(idx));
+          has = true;
+          st.sp = 0;
+          leaf = 0;
+          steps = 0;
+          node = empty ? kSentinel : root_ref(sc);
+        } else {
+          exhausted = true;
+        }
+      }
+    }
+    if (__all_sync(0xffffffffu, !has)) return;  // every lane is exhausted
+    do {
+      // A lane may start at, or come back to, a leaf with none postponed.
+      if (node < 0 && leaf == 0) {
+        leaf = node;
+        node = st.pop();
+      }
+      // Descend until every lane holds a leaf (or has finished).
+      while (node >= 0 && node != kSentinel) {
+        if (++steps > step_limit) {
+          status |= kStatusStepLimit;
+          node = kSentinel;
+          leaf = 0;
+          break;
+        }
+        const NodeRefs nd = load_node(sc.nodes, node);
+        const float tm = q.t_max();
+        const TravRay& r = q.ray();
+        const float e0 = box_entry(r, nd.lxy.x, nd.lxy.y, nd.lxy.z, nd.lxy.w, nd.lrz.x, nd.lrz.y, tm);
+        const float e1 = box_entry(r, nd.rxy.x, nd.rxy.y, nd.rxy.z, nd.rxy.w, nd.lrz.z, nd.lrz.w, tm);
+        const bool h0 = e0 >= 0.0f, h1 = e1 >= 0.0f;
+        if (!h0 && !h1) {
+          node = st.pop();
+        } else {
+          // Nearer child next, the other pushed. The far reference is
+          // derived from the near one by xor rather than by a second select
+          // on the same condition: nvcc 12.9 at -O1 and above merged such a
+          // select pair into one value, pushing the near child twice.
+          const int near_ref = (h0 && (!h1 || e0 <= e1)) ? nd.left : nd.right;
+          node = near_ref;
+          if (h0 && h1 && !st.push(nd.left ^ nd.right ^ near_ref)) status |= kStatusStackOverflow;
+        }
+        if (node < 0 && leaf == 0) {  // postpone the leaf, keep descending
+          leaf = node;
+          node = st.pop();
+        }
+        if (!__any_sync(__activemask(), leaf == 0)) break;
+      }
+      // Test the postponed leaf, then any leaf reached right after it.
+      while (leaf < 0) {
+        if (++steps > step_limit) {
+          status |= kStatusStepLimit;
+          node = kSentinel;
+          leaf = 0;
+          break;
+        }
+        if (!q.leaf(~leaf)) {
+          node = kSentinel;
+          leaf = 0;
+          st.sp = 0;
+          break;
+        }
+        leaf = 0;
+        if (node < 0) {
+          leaf = node;
+          node = st.pop();
+        }
+      }
+      if (has && node == kSentinel && leaf == 0) {
+        q.finish();
+        has = false;
+      }
+    } while (__popc(__ballot_sync(0xffffffffu, !has)) < kRefill && __any_sync(0xffffffffu, has));
+  }
+}
+
+// Closest hit of one query: intersectClosest, src/bvh.ts:202-282.
 struct ClosestHit {
   int tri;
   float t, u, v;
   bool front;
 };
 
-// intersectClosest, src/bvh.ts:202-282: nearest hit with side culling.
-MCRT_D ClosestHit trace_closest(const DScene& sc, const TravRay& r, bool cull, TravStack& st, unsigned& status) {
-  ClosestHit h{-1, 0.0f, 0.0f, 0.0f, true};
-  float t_max = __int_as_float(0x7f800000);
-  traverse(sc, r, t_max, st, status, [&](int first, int count, float& tm) {
-    for (int k = first; k < first + count; k++) {
+struct ClosestState {
+  TravRay r;
+  float tmax;
+  bool cull;
+  ClosestHit h;
+  MCRT_D void start(V3 o, V3 d, bool c) {
+    r = make_trav_ray(o, d);
+    tmax = __int_as_float(0x7f800000);
+    cull = c;
+    tests = 0;
+    h = ClosestHit{-1, 0.0f, 0.0f, 0.0f, true};
+  }
+  int tests;
+  MCRT_D bool leaf(const DScene& sc, int first) {
+    for (int k = first; k < sc.tri_count; k++) {
       V3 a, b, c;
       float4 w0, w1;
       load_tri(sc, k, a, b, c, w0, w1);
+      tests++;
       TriHit th;
-      if (intersect_triangle(r, a, b, c, tm, cull ? tri_side(w0.w) : 2, th)) {
-        tm = th.t;
-        h.tri = k;
-        h.t = th.t;
-        h.u = th.u;
-        h.v = th.v;
-        h.front = th.front;
+      if (intersect_triangle(r, a, b, c, tmax, cull ? tri_side(w0.w) : 2, th)) {
+        tmax = th.t;
+        h = ClosestHit{k, th.t, th.u, th.v, th.front};
       }
+      if (leaf_end(w0.w)) break;
     }
     return true;
-  });
-  return h;
-}
+  }
+};
 
 }  // namespace mcrt
