@@ -118,6 +118,27 @@ int32_t mcrt_intersect_closest(mcrt_executor* executor, int32_t geometry_version
                                const float* rays, int32_t cull, int32_t* triangle, float* t, float* u,
                                int32_t* front);
 
+/* mcrt_intersect_closest without allocating: the same query, arguments and
+ * results, for callers that must not allocate device memory during the call,
+ * such as a picking query issued between frames while renders run on other
+ * streams (cudaFree waits for all work on the device, and cudaMalloc may), or
+ * a process whose device memory is already handed to another allocator (a
+ * framework's caching pool), where a new allocation would fail. It has no
+ * counterpart in the reference.
+ *
+ * Its working memory (staged rays, hits, counters) is one fixed array per
+ * device, 4 MiB + 256 B, held by every GPU that loads this library until the
+ * process exits. At most 65,536 rays per call; a longer list is rejected
+ * with MCRT_ERR_LIMIT. The first call on each device looks up that device's
+ * array (a call with count 0 does only this); make it before any stream
+ * capture. All calls share the array, which keeps the last call's contents:
+ * overlapping calls on one device, from any executors or threads, race and
+ * must be serialised by the caller. The resident scene is the one uploaded
+ * earlier by mcrt_send_geometry. */
+int32_t mcrt_intersect_closest_noalloc(mcrt_executor* executor, int32_t geometry_version, int32_t count,
+                                       const float* rays, int32_t cull, int32_t* triangle, float* t, float* u,
+                                       int32_t* front);
+
 /* intersectAny, src/bvh.ts:289-332, with a counting visitor: the number of
  * triangles each ray hits between 0 and its limit (rays as above, the 4th
  * float a positive t limit or 0 for none). */

@@ -18,6 +18,9 @@ MCRT_ERR_NO_SCENE = 3
 MCRT_ERR_TEXTURE = 4
 MCRT_ERR_LIMIT = 5
 
+# Rays per call of mcrt_intersect_closest_noalloc (its fixed per-device array holds this many).
+NOALLOC_MAX_RAYS = 1 << 16
+
 
 class McrtError(RuntimeError):
     """A failed libmcrt call: `code` is the MCRT_ERR_* status."""
@@ -65,6 +68,8 @@ SIGNATURES = {
     "mcrt_trace_primary": (_i32, [_vp, _i32, _P(abi.mcrt_camera), _i32, _i32, _i32, _u32, _i32, _P(_i32), _P(_i32),
                                   _P(_i32), _P(_f), _P(_i32)]),
     "mcrt_intersect_closest": (_i32, [_vp, _i32, _i32, _P(_f), _i32, _P(_i32), _P(_f), _P(_f), _P(_i32)]),
+    "mcrt_intersect_closest_noalloc": (_i32, [_vp, _i32, _i32, _P(_f), _i32, _P(_i32), _P(_f), _P(_f),
+                                              _P(_i32)]),
     "mcrt_intersect_any_count": (_i32, [_vp, _i32, _i32, _P(_f), _P(_i32)]),
     "mcrt_build_bvh": (_i32, [_vp, _P(_f), _i32, _P(_f), _P(_i32), _P(_u32), _P(_i32)]),
     "mcrt_compile_geometry": (_i32, [_vp, _i32, _P(_d), _P(_d), _P(_d), _P(_d), _P(_u8), _P(_u32), _P(_u8), _P(_u8),

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
@@ -391,6 +392,60 @@ void check_index(int v, int count, const char* what) {
 }
 
 }  // namespace
+
+// ------------------------------------------------ statically held scratch
+// Working memory of mcrt_intersect_closest_noalloc, which allocates nothing:
+// one fixed array per device, created when the library's device code is
+// loaded there and held until the process exits. Offsets in bytes:
+//   [0, 256)           counters: work counter, walk status
+//   kNoAllocRaysAt     staged rays, 32 B each
+//   kNoAllocHitsAt     packed hits (triangle, t, u, front | tests << 8), 16 B each
+//   kNoAllocFieldsAt   the hits split per field: triangle, t, u, front, 4 B each
+// with room for kNoAllocMaxRays rays in every region (4 MiB + 256 B in all).
+static constexpr int kNoAllocMaxRays = 1 << 16;
+static constexpr size_t kNoAllocRaysAt = 256;
+static constexpr size_t kNoAllocHitsAt = kNoAllocRaysAt + 32 * static_cast<size_t>(kNoAllocMaxRays);
+static constexpr size_t kNoAllocFieldsAt = kNoAllocHitsAt + 16 * static_cast<size_t>(kNoAllocMaxRays);
+static constexpr size_t kNoAllocBytes = kNoAllocFieldsAt + 16 * static_cast<size_t>(kNoAllocMaxRays);
+
+static __device__ __align__(256) unsigned char g_query_scratch[kNoAllocBytes];
+
+namespace mcrt {
+namespace {
+
+// Splits packed closest hits into one array per field, so each field can be
+// copied straight into the caller's array.
+__global__ void k_split_hits(const int4* __restrict__ hits, int n, int* __restrict__ tri, float* __restrict__ t,
+                             float* __restrict__ u, int* __restrict__ front) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 h = hits[i];
+  tri[i] = h.x;
+  t[i] = __int_as_float(h.y);
+  u[i] = __int_as_float(h.z);
+  front[i] = h.w & 1;
+}
+
+// Device address of g_query_scratch on `device`, which must be current. In
+// host code the array's name stands for the variable, not for a device
+// address, so the address is asked of the runtime once per device (the
+// first call there) and kept.
+unsigned char* query_scratch(int device) {
+  constexpr int kDevices = 64;
+  static std::mutex mu;
+  static unsigned char* addr[kDevices] = {};
+  if (device < 0 || device >= kDevices) fail(MCRT_ERR_INVALID, "device index beyond the scratch table");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    void* p = nullptr;
+    cuda_check(cudaGetSymbolAddress(&p, g_query_scratch), "cudaGetSymbolAddress (query scratch)");
+    addr[device] = static_cast<unsigned char*>(p);
+  }
+  return addr[device];
+}
+
+}  // namespace
+}  // namespace mcrt
 
 // ====================================================================== ABI
 extern "C" {
@@ -855,6 +910,45 @@ int32_t mcrt_intersect_any_count(mcrt_executor* ex, int32_t gv, int32_t count, c
     unsigned* fetch = static_cast<unsigned*>(ex->scratch.ensure(sizeof(unsigned)));
     cuda_check(launch_count_hits(make_scene(ex), r, count, c, fetch, ex->stream), "trace");
     download(ex, counts, c, sizeof(int) * count, "download");
+  });
+}
+
+int32_t mcrt_intersect_closest_noalloc(mcrt_executor* ex, int32_t gv, int32_t count, const float* rays,
+                                       int32_t cull, int32_t* triangle, float* t, float* u, int32_t* front) {
+  return guard([&] {
+    checked(ex);
+    require_scene(ex, gv, 0, false);
+    if (count < 0 || (count > 0 && (!rays || !triangle))) fail(MCRT_ERR_INVALID, "bad ray list");
+    if (count > kNoAllocMaxRays)
+      fail(MCRT_ERR_LIMIT, "mcrt_intersect_closest_noalloc: " + std::to_string(count) +
+                               " rays exceed its limit of " + std::to_string(kNoAllocMaxRays) +
+                               " per call (split the list, or use mcrt_intersect_closest)");
+    unsigned char* base = query_scratch(ex->device);  // set-up on the device's first call
+    if (count == 0) return;
+    unsigned* counters = reinterpret_cast<unsigned*>(base);
+    float4* r = reinterpret_cast<float4*>(base + kNoAllocRaysAt);
+    int4* h = reinterpret_cast<int4*>(base + kNoAllocHitsAt);
+    int* f_tri = reinterpret_cast<int*>(base + kNoAllocFieldsAt);
+    float* f_t = reinterpret_cast<float*>(f_tri + kNoAllocMaxRays);
+    float* f_u = f_t + kNoAllocMaxRays;
+    int* f_front = reinterpret_cast<int*>(f_u + kNoAllocMaxRays);
+    const cudaStream_t s = ex->stream;
+    cuda_check(cudaMemcpyAsync(r, rays, sizeof(float) * 8 * count, cudaMemcpyHostToDevice, s), "upload");
+    // The array keeps the previous call's contents: the walk status starts
+    // at zero here, the work counter inside launch_trace_rays.
+    cuda_check(cudaMemsetAsync(counters + 1, 0, sizeof(unsigned), s), "memset");
+    cuda_check(launch_trace_rays(make_scene(ex), r, count, cull, h, counters, s), "trace");
+    k_split_hits<<<blocks(count, 256), 256, 0, s>>>(h, count, f_tri, f_t, f_u, f_front);
+    cuda_check(cudaGetLastError(), "split hits");
+    unsigned walk_status = 0;
+    const cudaMemcpyKind d2h = cudaMemcpyDeviceToHost;
+    cuda_check(cudaMemcpyAsync(&walk_status, counters + 1, sizeof(unsigned), d2h, s), "download");
+    cuda_check(cudaMemcpyAsync(triangle, f_tri, sizeof(int32_t) * count, d2h, s), "download");
+    if (t) cuda_check(cudaMemcpyAsync(t, f_t, sizeof(float) * count, d2h, s), "download");
+    if (u) cuda_check(cudaMemcpyAsync(u, f_u, sizeof(float) * count, d2h, s), "download");
+    if (front) cuda_check(cudaMemcpyAsync(front, f_front, sizeof(int32_t) * count, d2h, s), "download");
+    cuda_check(cudaStreamSynchronize(s), "download");
+    ex->stats.status |= walk_status;
   });
 }
 

@@ -28,7 +28,7 @@ from typing import Any, Dict, List, Optional, Sequence, Set, Tuple
 import numpy as np
 
 from . import abi
-from ._lib import McrtError, call, load, mcrt_stats
+from ._lib import NOALLOC_MAX_RAYS, McrtError, call, load, mcrt_stats
 from .types import (
     CompiledBvh,
     CompiledCamera,
@@ -251,6 +251,24 @@ class GpuExecutor:
         with self._lock:
             call("mcrt_intersect_closest", self._h, int(geometry_version), n, abi.ptr(rays, C.c_float), int(cull),
                  abi.ptr(tri, C.c_int32), abi.ptr(t, C.c_float), abi.ptr(u, C.c_float), abi.ptr(front, C.c_int32))
+        return {"tri": tri, "t": t, "u": u, "front": front}
+
+    def intersect_closest_noalloc(self, geometry_version: int, rays: np.ndarray, cull: bool = True
+                                  ) -> Dict[str, np.ndarray]:
+        """intersect_closest through mcrt_intersect_closest_noalloc: no device memory is allocated
+        during the call (working memory is the library's fixed per-device array), at most
+        NOALLOC_MAX_RAYS rays. The array is shared by every executor on the device, so calls from
+        different executors must not overlap; this executor's lock serialises its own calls."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        tri = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        u = np.zeros(n, np.float32)
+        front = np.zeros(n, np.int32)
+        with self._lock:
+            call("mcrt_intersect_closest_noalloc", self._h, int(geometry_version), n, abi.ptr(rays, C.c_float),
+                 int(cull), abi.ptr(tri, C.c_int32), abi.ptr(t, C.c_float), abi.ptr(u, C.c_float),
+                 abi.ptr(front, C.c_int32))
         return {"tri": tri, "t": t, "u": u, "front": front}
 
     def intersect_any_count(self, geometry_version: int, rays: np.ndarray) -> np.ndarray:
