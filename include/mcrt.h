@@ -174,6 +174,71 @@ int32_t mcrt_set_capacity(mcrt_executor* executor, int32_t paths);
 int32_t mcrt_get_stats(mcrt_executor* executor, mcrt_stats* out);
 int32_t mcrt_reset_stats(mcrt_executor* executor);
 
+/* ------------------------------------------------------------------------
+ * Batched and served rendering. No counterpart in the reference, whose
+ * ProgressiveRenderer (src/progressive.ts:177-282) schedules one render at a
+ * time over tile executors: here many progressive renders (scenes, cameras,
+ * sizes, sample counts) share one wavefront. Each request follows
+ * ProgressiveRenderer.render for a whole-image tile: an optional block preview
+ * written straight into the image, then `samples` passes accumulated in pass
+ * order, so the final image equals mcrt_raytrace's for the same inputs.
+ * ------------------------------------------------------------------------ */
+typedef struct mcrt_batch mcrt_batch;
+
+typedef struct mcrt_request {
+  mcrt_executor* scene;     /* executor whose resident scene is rendered (same device; keep it alive
+                               and unchanged while the request runs) */
+  int32_t geometry_version; /* versions the executor must hold (MCRT_ERR_NO_SCENE otherwise) */
+  int32_t shading_version;
+  mcrt_camera camera;
+  mcrt_settings settings;
+  int32_t width, height;
+  int32_t samples;          /* passes to accumulate (>= 1) */
+  int32_t preview_block;    /* > 1: a block preview first (ProgressiveOptions.previewBlock) */
+  int32_t srgb;             /* encode sRGB output */
+  uint8_t* image;           /* host RGBA8, width * height * 4, for the final image; or NULL */
+  uint8_t* preview_image;   /* host RGBA8 for the block preview; or NULL */
+} mcrt_request;
+
+enum { MCRT_EVENT_PREVIEW = 1, MCRT_EVENT_DONE = 2 };
+
+typedef struct mcrt_batch_event {
+  int64_t id;
+  int32_t kind;     /* MCRT_EVENT_*: preview_image / image (if given) hold the result */
+  int32_t samples;  /* passes accumulated */
+} mcrt_batch_event;
+
+typedef struct mcrt_batch_stats {
+  uint64_t closest_rays, any_rays, samples, chunks, graph_launches;
+  double gpu_ms;        /* device time of the chunks */
+  uint64_t arena_bytes; /* budget for request buffers (sums and images) */
+  uint64_t arena_used;
+  uint64_t path_bytes;  /* path pool */
+  uint32_t status;      /* kernel-reported limits hit (as mcrt_stats) */
+  uint32_t pad_;
+} mcrt_batch_stats;
+
+/* A batch renderer on `device`: `capacity` paths per chunk, `arena_bytes` of
+ * device memory for admitted requests' sums and images (admission waits for
+ * room), `use_graph` 1 to run each chunk's bounce loop as one CUDA graph with
+ * a while node, 0 for a host-driven loop. */
+int32_t mcrt_batch_create(int32_t device, int32_t capacity, int64_t arena_bytes, int32_t use_graph,
+                          mcrt_batch** out);
+int32_t mcrt_batch_destroy(mcrt_batch* batch);
+/* Paths per chunk (<= capacity); smaller chunks bound preview latency. */
+int32_t mcrt_batch_set_chunk(mcrt_batch* batch, int32_t paths);
+/* Queues a request; *id identifies it in events. */
+int32_t mcrt_batch_submit(mcrt_batch* batch, const mcrt_request* request, int64_t* id);
+/* Stops a request (a camera move restarts it as a new request). */
+int32_t mcrt_batch_cancel(mcrt_batch* batch, int64_t id);
+/* Launches the next chunk, waits for the previous one and returns up to
+ * max_events events; *idle is 1 when nothing is queued or in flight. */
+int32_t mcrt_batch_step(mcrt_batch* batch, mcrt_batch_event* events, int32_t max_events, int32_t* n_events,
+                        int32_t* idle);
+/* Submits `count` requests and runs until all are done. */
+int32_t mcrt_batch_render(mcrt_batch* batch, int32_t count, const mcrt_request* requests);
+int32_t mcrt_batch_get_stats(mcrt_batch* batch, mcrt_batch_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,6 +71,14 @@ SIGNATURES = {
     "mcrt_intersect_closest_noalloc": (_i32, [_vp, _i32, _i32, _P(_f), _i32, _P(_i32), _P(_f), _P(_f),
                                               _P(_i32)]),
     "mcrt_intersect_any_count": (_i32, [_vp, _i32, _i32, _P(_f), _P(_i32)]),
+    "mcrt_batch_create": (_i32, [_i32, _i32, C.c_int64, _i32, _P(_vp)]),
+    "mcrt_batch_destroy": (_i32, [_vp]),
+    "mcrt_batch_set_chunk": (_i32, [_vp, _i32]),
+    "mcrt_batch_submit": (_i32, [_vp, _vp, _P(C.c_int64)]),
+    "mcrt_batch_cancel": (_i32, [_vp, C.c_int64]),
+    "mcrt_batch_step": (_i32, [_vp, _vp, _i32, _P(_i32), _P(_i32)]),
+    "mcrt_batch_render": (_i32, [_vp, _i32, _vp]),
+    "mcrt_batch_get_stats": (_i32, [_vp, _vp]),
     "mcrt_build_bvh": (_i32, [_vp, _P(_f), _i32, _P(_f), _P(_i32), _P(_u32), _P(_i32)]),
     "mcrt_compile_geometry": (_i32, [_vp, _i32, _P(_d), _P(_d), _P(_d), _P(_d), _P(_u8), _P(_u32), _P(_u8), _P(_u8),
                                      _P(_f), _P(_f), _P(_f), _P(_f), _P(_f), _P(_u32), _P(_u8), _P(_u8), _P(_f),

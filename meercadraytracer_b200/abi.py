@@ -127,6 +127,29 @@ class mcrt_tile(C.Structure):
     _fields_ = [("x", C.c_int32), ("y", C.c_int32), ("width", C.c_int32), ("height", C.c_int32)]
 
 
+class mcrt_request(C.Structure):
+    """A batched render request (include/mcrt.h)."""
+
+    _fields_ = [
+        ("scene", C.c_void_p), ("geometry_version", C.c_int32), ("shading_version", C.c_int32),
+        ("camera", mcrt_camera), ("settings", mcrt_settings), ("width", C.c_int32), ("height", C.c_int32),
+        ("samples", C.c_int32), ("preview_block", C.c_int32), ("srgb", C.c_int32),
+        ("image", C.POINTER(C.c_uint8)), ("preview_image", C.POINTER(C.c_uint8)),
+    ]
+
+
+class mcrt_batch_event(C.Structure):
+    _fields_ = [("id", C.c_int64), ("kind", C.c_int32), ("samples", C.c_int32)]
+
+
+class mcrt_batch_stats(C.Structure):
+    _fields_ = [
+        ("closest_rays", C.c_uint64), ("any_rays", C.c_uint64), ("samples", C.c_uint64), ("chunks", C.c_uint64),
+        ("graph_launches", C.c_uint64), ("gpu_ms", C.c_double), ("arena_bytes", C.c_uint64),
+        ("arena_used", C.c_uint64), ("path_bytes", C.c_uint64), ("status", C.c_uint32), ("pad_", C.c_uint32),
+    ]
+
+
 def ptr(array: np.ndarray, ctype: Any) -> Any:
     """Pointer to a C-contiguous numpy array's data, or NULL for an empty array."""
     if array is None or array.size == 0:

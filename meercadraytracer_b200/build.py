@@ -25,9 +25,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = {
     "render.cu": [],
     "executor.cu": [],
+    "batch.cu": [],
     "scene_build.cu": ["--fmad=false"],
 }
-HEADERS = ["mcrt_math.cuh", "device_scene.cuh", "traverse.cuh", "render.cuh", "scene_build.cuh", "dfg_lut.h"]
+HEADERS = ["mcrt_math.cuh", "device_scene.cuh", "traverse.cuh", "render.cuh", "scene_build.cuh", "batch.cuh", "dfg_lut.h"]
 
 
 def nvcc() -> str:

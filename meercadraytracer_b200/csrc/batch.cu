@@ -1,0 +1,455 @@
+// Batched and served rendering (batch.cuh): chunk planning, admission, the
+// per-chunk CUDA graph and completion events.
+#include "batch.cuh"
+
+#include <algorithm>
+#include <cstddef>
+#include <cstring>
+#include <iterator>
+
+namespace mcrt {
+
+// ------------------------------------------------------------------ arena
+DeviceArena::~DeviceArena() {
+  if (base_) cudaFree(base_);
+}
+
+cudaError_t DeviceArena::init(size_t bytes) {
+  bytes = std::max<size_t>(bytes, 256) & ~static_cast<size_t>(255);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&base_), bytes);
+  if (e != cudaSuccess) {
+    base_ = nullptr;
+    return e;
+  }
+  size_ = bytes;
+  free_.clear();
+  live_.clear();
+  free_[0] = bytes;
+  used_ = 0;
+  return cudaSuccess;
+}
+
+void* DeviceArena::alloc(size_t bytes) {
+  bytes = (std::max<size_t>(bytes, 1) + 255) & ~static_cast<size_t>(255);
+  for (auto it = free_.begin(); it != free_.end(); ++it) {
+    if (it->second < bytes) continue;
+    const size_t off = it->first, len = it->second;
+    free_.erase(it);
+    if (len > bytes) free_[off + bytes] = len - bytes;
+    live_[off] = bytes;
+    used_ += bytes;
+    return base_ + off;
+  }
+  return nullptr;
+}
+
+void DeviceArena::free(void* p) {
+  if (!p) return;
+  const size_t off = static_cast<size_t>(static_cast<char*>(p) - base_);
+  auto it = live_.find(off);
+  if (it == live_.end()) return;
+  size_t start = off, len = it->second;
+  used_ -= len;
+  live_.erase(it);
+  auto next = free_.lower_bound(start);
+  if (next != free_.end() && next->first == start + len) {  // merge with the block after
+    len += next->second;
+    next = free_.erase(next);
+  }
+  if (next != free_.begin()) {  // and with the block before
+    auto prev = std::prev(next);
+    if (prev->first + prev->second == start) {
+      start = prev->first;
+      len += prev->second;
+      free_.erase(prev);
+    }
+  }
+  free_[start] = len;
+}
+
+// ----------------------------------------------------------------- engine
+BatchEngine::~BatchEngine() {
+  cudaSetDevice(device_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  if (copy_stream_) cudaStreamSynchronize(copy_stream_);
+  for (Chunk& c : inflight_) {
+    if (c.start) cudaEventDestroy(c.start);
+    if (c.done) cudaEventDestroy(c.done);
+    if (c.copied) cudaEventDestroy(c.copied);
+  }
+  destroy_graph();
+  if (tables_dev_) cudaFree(tables_dev_);
+  for (BatchTables* t : tables_host_)
+    if (t) cudaFreeHost(t);
+  if (counters_dev_) cudaFree(counters_dev_);
+  if (counters_host_) cudaFreeHost(counters_host_);
+  if (stream_) cudaStreamDestroy(stream_);
+  if (copy_stream_) cudaStreamDestroy(copy_stream_);
+}
+
+cudaError_t BatchEngine::init(int device, int capacity, size_t arena_bytes, bool use_graph) {
+  device_ = device;
+  capacity_ = std::max(capacity, 1);
+  use_graph_ = use_graph;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = arena_.init(arena_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&tables_dev_), sizeof(BatchTables));
+  for (int i = 0; i < 2 && e == cudaSuccess; i++)
+    e = cudaMallocHost(reinterpret_cast<void**>(&tables_host_[i]), sizeof(BatchTables));
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&counters_dev_), sizeof(BatchCounters));
+  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&counters_host_), sizeof(BatchCounters));
+  if (e == cudaSuccess) e = cudaMemset(counters_dev_, 0, sizeof(BatchCounters));
+  if (e == cudaSuccess) e = cudaMemset(tables_dev_, 0, sizeof(BatchTables));
+  if (e == cudaSuccess) e = paths_.reserve(capacity_, slots_);
+  if (e == cudaSuccess) e = batch_grids(&grids_);
+  return e;
+}
+
+bool BatchEngine::scene_busy(int slot) const {
+  for (const auto& r : requests_)
+    if (r->d.scene == slot && (!r->finished || r->inflight > 0) && !(r->cancelled && r->inflight == 0)) return true;
+  return false;
+}
+
+cudaError_t BatchEngine::set_scene(int slot, const DScene& scene, int lights) {
+  if (slot < 0 || slot >= kMaxBatchScenes || lights < 0) return cudaErrorInvalidValue;
+  if (scene_busy(slot)) return cudaErrorNotReady;
+  cudaSetDevice(device_);
+  // Chunks in flight keep the old graph and path state: wait for them.
+  cudaError_t e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) return e;
+  scenes_[slot] = scene;
+  lights_[slot] = lights;
+  scene_set_[slot] = true;
+  nscenes_ = std::max(nscenes_, slot + 1);
+  int slots = 1;
+  for (int i = 0; i < nscenes_; i++)
+    if (scene_set_[i]) slots = std::max(slots, lights_[i] + 1);
+  if (slots > paths_.slots()) {
+    e = paths_.reserve(capacity_, slots);
+    if (e != cudaSuccess) return e;
+  }
+  slots_ = std::max(slots_, slots);
+  graph_valid_ = false;
+  return cudaSuccess;
+}
+
+void BatchEngine::destroy_graph() {
+  if (exec_) cudaGraphExecDestroy(exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  exec_ = nullptr;
+  graph_ = nullptr;
+  graph_valid_ = false;
+}
+
+// One graph per scene set: raygen, a while node around the bounce iteration
+// (its last kernel sets the condition), then accumulate. Every kernel reads
+// the chunk from tables_dev_, so the graph is reused by every chunk.
+cudaError_t BatchEngine::ensure_graph() {
+  if (!use_graph_ || graph_valid_) return cudaSuccess;
+  destroy_graph();
+  const PathState ps = paths_.state();
+  const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+  cudaError_t e = cudaGraphCreate(&graph_, 0);
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(stream_, graph_, nullptr, nullptr, 0, mode);
+  if (e != cudaSuccess) return e;
+  cudaError_t le = launch_batch_raygen(tables_dev_, ps, grids_, stream_);
+  e = cudaStreamEndCapture(stream_, &graph_);
+  if (e == cudaSuccess) e = le;
+  if (e != cudaSuccess) return e;
+  size_t n = 0;
+  e = cudaGraphGetNodes(graph_, nullptr, &n);
+  if (e != cudaSuccess) return e;
+  std::vector<cudaGraphNode_t> roots(n);
+  if (n > 0) e = cudaGraphGetNodes(graph_, roots.data(), &n);
+  cudaGraphConditionalHandle handle = 0;
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, graph_, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) return e;
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = handle;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t loop = nullptr;
+  e = cudaGraphAddNode(&loop, graph_, roots.data(), n, &p);
+  if (e != cudaSuccess) return e;
+  cudaGraph_t body = p.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, mode);
+  if (e != cudaSuccess) return e;
+  le = launch_batch_iteration(scenes_, nscenes_, tables_dev_, ps, paths_.capacity(), paths_.slots(), counters_dev_,
+                              grids_, true, handle, stream_);
+  e = cudaStreamEndCapture(stream_, &body);
+  if (e == cudaSuccess) e = le;
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(stream_, graph_, &loop, nullptr, 1, mode);
+  if (e != cudaSuccess) return e;
+  le = launch_batch_accumulate(tables_dev_, ps, grids_, stream_);
+  e = cudaStreamEndCapture(stream_, &graph_);
+  if (e == cudaSuccess) e = le;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec_, graph_, 0);
+  if (e == cudaSuccess) graph_valid_ = true;
+  return e;
+}
+
+long long BatchEngine::submit(const BatchRequestDesc& d, uint8_t* host_image, uint8_t* host_preview) {
+  if (d.scene < 0 || d.scene >= kMaxBatchScenes || !scene_set_[d.scene]) return -1;
+  if (d.fp.width <= 0 || d.fp.height <= 0 || d.samples < 1) return -1;
+  auto r = std::make_unique<Request>();
+  r->id = next_id_++;
+  r->d = d;
+  r->host_image = host_image;
+  r->host_preview = host_preview;
+  r->preview = d.preview_block > 1 ? 1 : 0;
+  const long long id = r->id;
+  requests_.push_back(std::move(r));
+  return id;
+}
+
+bool BatchEngine::cancel(long long id) {
+  for (auto it = requests_.begin(); it != requests_.end(); ++it) {
+    Request& r = **it;
+    if (r.id != id || r.cancelled || r.finished) continue;
+    r.cancelled = true;
+    if (r.inflight == 0) {
+      release(r);
+      requests_.erase(it);
+    }
+    return true;
+  }
+  return false;
+}
+
+void BatchEngine::release(Request& r) {
+  if (r.sum) arena_.free(r.sum);
+  r.sum = nullptr;
+  r.image = nullptr;
+}
+
+bool BatchEngine::admit(Request& r) {
+  const size_t pix = static_cast<size_t>(r.pixels());
+  const size_t sum_bytes = (pix * sizeof(float4) + 255) & ~static_cast<size_t>(255);
+  void* p = arena_.alloc(sum_bytes + pix * 4);
+  if (!p) return false;
+  r.sum = static_cast<float4*>(p);
+  r.image = static_cast<uint8_t*>(p) + sum_bytes;
+  cudaMemsetAsync(r.sum, 0, pix * sizeof(float4), stream_);
+  r.admitted = true;
+  return true;
+}
+
+// Chooses the chunk's segments: admissions in submission order while the
+// arena has room, previews first, then passes of the admitted requests in
+// submission order, each request at most once.
+void BatchEngine::plan(Chunk& c) {
+  long long room = chunk_paths_ > 0 ? std::min(chunk_paths_, capacity_) : capacity_;
+  for (auto& rp : requests_) {
+    Request& r = *rp;
+    if (r.admitted || r.cancelled) continue;
+    if (!admit(r)) break;  // no overtaking: later requests wait too
+  }
+  std::vector<Request*> used;
+  auto take = [&](Request& r, int preview, int pass0, int passes, int pix0, int npix) {
+    SegmentPlan s{&r, preview, pass0, passes, pix0, npix, preview ? 0 : pass0 + passes};
+    c.segs.push_back(s);
+    used.push_back(&r);
+    room -= static_cast<long long>(npix) * passes;
+  };
+  auto active = [](const Request& r) { return r.admitted && !r.cancelled && !r.finished; };
+  for (auto& rp : requests_) {
+    Request& r = *rp;
+    if (!active(r) || r.preview != 1 || static_cast<int>(c.segs.size()) >= kMaxSegments) continue;
+    const int b = r.d.preview_block;
+    const long long blocks = static_cast<long long>((r.d.fp.width + b - 1) / b) * ((r.d.fp.height + b - 1) / b);
+    if (blocks > room) continue;
+    take(r, 1, 0, 1, 0, static_cast<int>(blocks));
+    r.preview = 2;
+  }
+  for (auto& rp : requests_) {
+    Request& r = *rp;
+    if (!active(r) || r.preview == 1 || static_cast<int>(c.segs.size()) >= kMaxSegments) continue;
+    if (std::find(used.begin(), used.end(), &r) != used.end()) continue;
+    if (r.next_pass >= r.d.samples || room <= 0) continue;
+    const long long P = r.pixels();
+    if (r.next_pix > 0 || P > capacity_) {
+      // A pass larger than the pool, or one already split: the next pixel range.
+      const int n = static_cast<int>(std::min<long long>(room, P - r.next_pix));
+      if (n <= 0) continue;
+      take(r, 0, r.next_pass, 1, r.next_pix, n);
+      r.next_pix += n;
+      if (r.next_pix >= P) {
+        r.next_pix = 0;
+        r.next_pass++;
+      }
+    } else if (P <= room) {
+      const int k = static_cast<int>(std::min<long long>(r.d.samples - r.next_pass, room / P));
+      take(r, 0, r.next_pass, k, 0, static_cast<int>(P));
+      r.next_pass += k;
+    }
+  }
+  // Scene-major order: each scene's paths form one range.
+  std::stable_sort(c.segs.begin(), c.segs.end(),
+                   [](const SegmentPlan& a, const SegmentPlan& b) { return a.r->d.scene < b.r->d.scene; });
+  for (SegmentPlan& s : c.segs) s.r->inflight++;
+}
+
+cudaError_t BatchEngine::launch(Chunk& c) {
+  BatchTables* T = tables_host_[c.slot];
+  const int nseg = static_cast<int>(c.segs.size());
+  T->segments = nseg;
+  T->iteration = 0;
+  int max_bounces = 0;
+  std::memset(T->scenes, 0, sizeof(T->scenes));
+  int paths = 0, items = 0;
+  for (int j = 0; j < nseg; j++) {
+    const SegmentPlan& s = c.segs[j];
+    const Request& r = *s.r;
+    FrameParams fp = r.d.fp;
+    fp.mode = 0;
+    fp.tile_x = fp.tile_y = 0;
+    fp.tile_w = fp.width;
+    fp.tile_h = fp.height;
+    fp.block = s.preview ? r.d.preview_block : 1;
+    fp.nbx = (fp.width + fp.block - 1) / fp.block;
+    fp.pass0 = s.pass0;
+    fp.pix0 = s.pix0;
+    fp.npix = s.npix;
+    fp.path_base = paths;
+    fp.capacity = paths_.capacity();
+    fp.slot_count = paths_.slots();
+    T->fp[j] = fp;
+    T->seg_base[j] = paths;
+    T->pix_base[j] = items;
+    SegmentOut& o = T->out[j];
+    o.sum = r.sum;
+    o.image = r.image;
+    o.passes = s.passes;
+    o.done_after = s.done_after;
+    o.preview = s.preview;
+    o.srgb = r.d.srgb;
+    SceneQueues& q = T->scenes[r.d.scene];
+    if (q.paths == 0) q.base = static_cast<unsigned>(paths);
+    q.paths += static_cast<unsigned>(s.npix * s.passes);
+    paths += s.npix * s.passes;
+    items += s.npix;
+    max_bounces = std::max(max_bounces, fp.max_bounces);
+    totals_.samples += static_cast<unsigned long long>(s.npix) * s.passes;
+  }
+  for (int i = 0; i < kMaxBatchScenes; i++) T->scenes[i].count = T->scenes[i].paths;
+  T->seg_base[nseg] = paths;
+  T->pix_base[nseg] = items;
+  T->paths = paths;
+  // Paths end by bounce count or after kMaxPassThrough pass-throughs per bounce.
+  T->max_iterations = (max_bounces + 1) * (kMaxPassThrough + 1) + 2;
+  const size_t bytes = offsetof(BatchTables, fp) + sizeof(FrameParams) * static_cast<size_t>(nseg);
+
+  cudaError_t e = cudaSuccess;
+  if (!c.start) e = cudaEventCreate(&c.start);
+  if (e == cudaSuccess && !c.done) e = cudaEventCreate(&c.done);
+  if (e == cudaSuccess && !c.copied) e = cudaEventCreateWithFlags(&c.copied, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = ensure_graph();
+  if (e == cudaSuccess) e = cudaEventRecord(c.start, stream_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tables_dev_, T, bytes, cudaMemcpyHostToDevice, stream_);
+  if (e != cudaSuccess) return e;
+  const PathState ps = paths_.state();
+  if (use_graph_) {
+    e = cudaGraphLaunch(exec_, stream_);
+    totals_.graph_launches++;
+  } else {
+    e = launch_batch_raygen(tables_dev_, ps, grids_, stream_);
+    for (int it = 0; e == cudaSuccess && it < T->max_iterations; it++) {
+      e = launch_batch_iteration(scenes_, nscenes_, tables_dev_, ps, paths_.capacity(), paths_.slots(), counters_dev_,
+                                 grids_, false, 0, stream_);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(counters_host_, counters_dev_, sizeof(BatchCounters), cudaMemcpyDeviceToHost, stream_);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+      if (e == cudaSuccess && !counters_host_->more) break;
+    }
+    if (e == cudaSuccess) e = launch_batch_accumulate(tables_dev_, ps, grids_, stream_);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(c.done, stream_);
+  if (e != cudaSuccess) return e;
+  totals_.chunks++;
+  // Images a request's client is waiting for: its preview, and the final image.
+  c.copies = false;
+  for (const SegmentPlan& s : c.segs) {
+    const Request& r = *s.r;
+    const bool last = !s.preview && s.pass0 + s.passes == r.d.samples && s.pix0 + s.npix == r.pixels();
+    uint8_t* dst = s.preview ? r.host_preview : (last ? r.host_image : nullptr);
+    if (!dst) continue;
+    if (!c.copies) e = cudaStreamWaitEvent(copy_stream_, c.done, 0);
+    c.copies = true;
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(dst, r.image, static_cast<size_t>(r.pixels()) * 4, cudaMemcpyDeviceToHost, copy_stream_);
+  }
+  if (e == cudaSuccess && c.copies) e = cudaEventRecord(c.copied, copy_stream_);
+  return e;
+}
+
+cudaError_t BatchEngine::finish(Chunk& c, std::vector<BatchEvent>& events) {
+  cudaError_t e = cudaEventSynchronize(c.done);
+  if (e == cudaSuccess && c.copies) e = cudaEventSynchronize(c.copied);
+  if (e != cudaSuccess) return e;
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, c.start, c.done) == cudaSuccess) totals_.gpu_ms += ms;
+  e = cudaMemcpy(counters_host_, counters_dev_, sizeof(BatchCounters), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return e;
+  totals_.closest = counters_host_->closest;
+  totals_.any = counters_host_->any;
+  totals_.status |= counters_host_->status;
+  for (const SegmentPlan& s : c.segs) {
+    Request& r = *s.r;
+    r.inflight--;
+    if (r.cancelled) continue;
+    if (s.preview) {
+      events.push_back(BatchEvent{r.id, kEventPreview, 0});
+    } else if (s.pass0 + s.passes == r.d.samples && s.pix0 + s.npix == r.pixels()) {
+      r.finished = true;
+      events.push_back(BatchEvent{r.id, kEventDone, r.d.samples});
+    }
+  }
+  for (auto it = requests_.begin(); it != requests_.end();) {
+    Request& r = **it;
+    if ((r.finished || r.cancelled) && r.inflight == 0) {
+      release(r);
+      it = requests_.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  return cudaSuccess;
+}
+
+cudaError_t BatchEngine::step(std::vector<BatchEvent>& events, bool* idle) {
+  cudaError_t e = cudaSetDevice(device_);
+  if (e != cudaSuccess) return e;
+  bool launched = false;
+  if (inflight_.size() < 2) {
+    Chunk c;
+    c.slot = next_slot_;
+    plan(c);
+    if (!c.segs.empty()) {
+      next_slot_ ^= 1;
+      inflight_.push_back(std::move(c));
+      e = launch(inflight_.back());
+      if (e != cudaSuccess) return e;
+      launched = true;
+    }
+  }
+  if (!inflight_.empty() && (inflight_.size() == 2 || !launched)) {
+    e = finish(inflight_.front(), events);
+    Chunk& done = inflight_.front();
+    if (done.start) cudaEventDestroy(done.start);
+    if (done.done) cudaEventDestroy(done.done);
+    if (done.copied) cudaEventDestroy(done.copied);
+    inflight_.pop_front();
+    if (e != cudaSuccess) return e;
+  }
+  bool pending = false;
+  for (const auto& r : requests_)
+    if (!r->cancelled && !r->finished) pending = true;
+  if (idle) *idle = !pending && inflight_.empty();
+  return cudaSuccess;
+}
+
+}  // namespace mcrt

@@ -1,0 +1,161 @@
+// Batched and served rendering: many progressive render requests (scenes,
+// cameras, sizes, sample counts) traced together in one wavefront over a
+// shared path pool, with admission by a device-memory budget.
+//
+// A request follows ProgressiveRenderer.render (src/progressive.ts:189-282)
+// for a whole-image tile: an optional block preview written straight into the
+// image, then `samples` passes accumulated in pass order into a Float32 running
+// sum, the image re-encoded after each chunk (writeTile, progressive.ts:288-313).
+// Each pass traces exactly the paths raytraceCompiled (src/raytrace.ts:69-82)
+// traces, so a request's image is the same alone and in any mix.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "render.cuh"
+
+namespace mcrt {
+
+// First-fit allocator over one device allocation (request sums and images), so
+// admitting and retiring requests never calls cudaMalloc or cudaFree, which
+// would synchronise the device.
+class DeviceArena {
+ public:
+  ~DeviceArena();
+  cudaError_t init(size_t bytes);
+  // Offset-aligned block of `bytes`, or nullptr when it does not fit now.
+  void* alloc(size_t bytes);
+  void free(void* p);
+  size_t capacity() const { return size_; }
+  size_t used() const { return used_; }
+
+ private:
+  char* base_ = nullptr;
+  size_t size_ = 0, used_ = 0;
+  std::map<size_t, size_t> free_;  // offset -> length
+  std::map<size_t, size_t> live_;  // offset -> length
+};
+
+struct BatchRequestDesc {
+  int scene = 0;          // scene slot
+  FrameParams fp{};       // camera, settings and image size; mode 0, whole image
+  int samples = 1;        // passes to accumulate
+  int preview_block = 0;  // > 1: a block preview first (ProgressiveOptions.previewBlock)
+  int srgb = 1;
+};
+
+enum BatchEventKind { kEventPreview = 1, kEventDone = 2, kEventFailed = 3 };
+
+struct BatchEvent {
+  long long id;
+  int kind;
+  int samples;  // passes accumulated when the event was raised
+};
+
+struct BatchTotals {
+  unsigned long long closest = 0, any = 0, samples = 0, chunks = 0, graph_launches = 0;
+  unsigned status = 0;
+  double gpu_ms = 0;  // device time of the chunks (events around each chunk)
+};
+
+class BatchEngine {
+ public:
+  BatchEngine() = default;
+  ~BatchEngine();
+  BatchEngine(const BatchEngine&) = delete;
+  BatchEngine& operator=(const BatchEngine&) = delete;
+
+  // `capacity`: paths per chunk; `arena_bytes`: budget for the requests'
+  // sums and images; `use_graph`: run each chunk's bounce loop as a CUDA
+  // graph with a while node (else a host-driven loop, one sync per bounce).
+  cudaError_t init(int device, int capacity, size_t arena_bytes, bool use_graph);
+  // Puts a scene into `slot` (< kMaxBatchScenes) with `lights` lights. Fails
+  // while requests on the slot are unfinished.
+  cudaError_t set_scene(int slot, const DScene& scene, int lights);
+  bool scene_busy(int slot) const;
+  // Queues a request; its buffers are taken from the arena when it is admitted.
+  long long submit(const BatchRequestDesc& d, uint8_t* host_image, uint8_t* host_preview);
+  // Stops a request; its buffers return to the arena once no chunk uses them.
+  bool cancel(long long id);
+  // Launches the next chunk (if any request has work), then waits for the
+  // chunk before it and appends the events it completed. *idle: nothing is
+  // queued, active or in flight.
+  cudaError_t step(std::vector<BatchEvent>& events, bool* idle);
+  BatchTotals totals() const { return totals_; }
+  int capacity() const { return capacity_; }
+  size_t path_bytes() const { return paths_.bytes(); }
+  const DeviceArena& arena() const { return arena_; }
+  cudaStream_t stream() const { return stream_; }
+  // Limits a chunk to `paths` paths (<= capacity): smaller chunks bound the
+  // latency of a new request's preview under load.
+  void set_chunk_paths(int paths) { chunk_paths_ = paths; }
+
+ private:
+  struct Request {
+    long long id;
+    BatchRequestDesc d;
+    uint8_t* host_image = nullptr;    // final image
+    uint8_t* host_preview = nullptr;  // block preview
+    float4* sum = nullptr;
+    uint8_t* image = nullptr;
+    bool admitted = false, cancelled = false, finished = false;
+    int preview = 0;          // 0 none, 1 to schedule, 2 scheduled
+    int next_pass = 0;        // first pass not yet scheduled
+    int next_pix = 0;         // first pixel of next_pass not yet scheduled (split passes)
+    int inflight = 0;         // chunks in flight that hold a segment of this request
+    long long pixels() const { return static_cast<long long>(d.fp.width) * d.fp.height; }
+  };
+  struct SegmentPlan {
+    Request* r;
+    int preview;
+    int pass0, passes, pix0, npix, done_after;
+  };
+  struct Chunk {
+    int slot;  // pinned table buffer
+    std::vector<SegmentPlan> segs;
+    cudaEvent_t start = nullptr, done = nullptr, copied = nullptr;
+    bool copies = false;
+  };
+
+  cudaError_t ensure_graph();
+  void destroy_graph();
+  bool admit(Request& r);
+  void plan(Chunk& c);
+  cudaError_t launch(Chunk& c);
+  cudaError_t finish(Chunk& c, std::vector<BatchEvent>& events);
+  void release(Request& r);
+
+  int device_ = 0;
+  int capacity_ = 0, chunk_paths_ = 0;
+  int slots_ = 1;
+  bool use_graph_ = true;
+  cudaStream_t stream_ = nullptr, copy_stream_ = nullptr;
+  PathBuffers paths_;
+  DeviceArena arena_;
+  BatchTables* tables_dev_ = nullptr;
+  BatchTables* tables_host_[2] = {nullptr, nullptr};
+  BatchCounters* counters_dev_ = nullptr;
+  BatchCounters* counters_host_ = nullptr;
+  BatchGrids grids_{};
+  DScene scenes_[kMaxBatchScenes]{};
+  int lights_[kMaxBatchScenes]{};
+  bool scene_set_[kMaxBatchScenes]{};
+  int nscenes_ = 0;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
+  bool graph_valid_ = false;
+  long long next_id_ = 1;
+  std::deque<std::unique_ptr<Request>> requests_;  // submission order
+  std::deque<Chunk> inflight_;
+  int next_slot_ = 0;
+  BatchTotals totals_;
+};
+
+}  // namespace mcrt

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <deque>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -20,6 +21,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "batch.cuh"
 #include "dfg_lut.h"
 #include "mcrt.h"
 #include "render.cuh"
@@ -1033,6 +1035,193 @@ int32_t mcrt_reset_stats(mcrt_executor* ex) {
     checked(ex);
     ex->stats = RenderStats{};
     ex->ms_total = 0;
+  });
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ batch renders
+// A batch renderer maps each (executor, geometry version, shading version)
+// its requests name to one of the engine's scene slots.
+struct mcrt_batch {
+  int device = 0;
+  BatchEngine engine;
+  struct Slot {
+    mcrt_executor* ex = nullptr;
+    int32_t gv = 0, sv = 0;
+    bool used = false;
+  } slots[kMaxBatchScenes];
+  std::deque<BatchEvent> pending;
+};
+
+namespace {
+
+mcrt_batch* checked_batch(mcrt_batch* b) {
+  if (!b) fail(MCRT_ERR_INVALID, "batch is NULL");
+  cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
+  return b;
+}
+
+// Fails when a slot's executor no longer holds the scene its unfinished
+// requests were submitted for.
+void check_slots(mcrt_batch* b) {
+  for (int i = 0; i < kMaxBatchScenes; i++) {
+    const auto& s = b->slots[i];
+    if (!s.used || !b->engine.scene_busy(i)) continue;
+    if (!s.ex->have_geometry || !s.ex->have_shading || s.ex->geometry_version != s.gv ||
+        s.ex->shading_version != s.sv)
+      fail(MCRT_ERR_NO_SCENE, "a batched request's executor changed its scene before the request finished");
+  }
+}
+
+int scene_slot(mcrt_batch* b, const mcrt_request* r) {
+  for (int i = 0; i < kMaxBatchScenes; i++) {
+    const auto& s = b->slots[i];
+    if (s.used && s.ex == r->scene && s.gv == r->geometry_version && s.sv == r->shading_version) return i;
+  }
+  int slot = -1;
+  for (int i = 0; i < kMaxBatchScenes && slot < 0; i++)
+    if (!b->slots[i].used) slot = i;
+  for (int i = 0; i < kMaxBatchScenes && slot < 0; i++)
+    if (!b->engine.scene_busy(i)) slot = i;
+  if (slot < 0) fail(MCRT_ERR_LIMIT, "a batch holds at most 8 scenes with unfinished requests");
+  cuda_check(b->engine.set_scene(slot, make_scene(r->scene), r->scene->sh.light_count), "batch scene");
+  b->slots[slot] = mcrt_batch::Slot{r->scene, r->geometry_version, r->shading_version, true};
+  return slot;
+}
+
+int64_t submit_request(mcrt_batch* b, const mcrt_request* r) {
+  if (!r || !r->scene) fail(MCRT_ERR_INVALID, "request or its scene is NULL");
+  if (r->scene->device != b->device) fail(MCRT_ERR_INVALID, "the request's executor is on another device");
+  set_device(r->scene);
+  require_scene(r->scene, r->geometry_version, r->shading_version, true);
+  cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
+  if (r->samples < 1) fail(MCRT_ERR_INVALID, "samples must be at least 1");
+  if (static_cast<long long>(r->width) * r->height > INT_MAX / 4) fail(MCRT_ERR_LIMIT, "image too large");
+  BatchRequestDesc d;
+  d.fp = frame_params(&r->camera, &r->settings, r->width, r->height);
+  d.samples = r->samples;
+  d.preview_block = r->preview_block > 1 ? r->preview_block : 0;
+  d.srgb = r->srgb ? 1 : 0;
+  const size_t pix = static_cast<size_t>(r->width) * r->height;
+  if (pix * 20 + 512 > b->engine.arena().capacity())
+    fail(MCRT_ERR_LIMIT, "the request's buffers exceed the batch's memory budget");
+  d.scene = scene_slot(b, r);
+  const long long id = b->engine.submit(d, r->image, r->preview_image);
+  if (id < 0) fail(MCRT_ERR_INVALID, "request rejected");
+  return id;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t mcrt_batch_create(int32_t device, int32_t capacity, int64_t arena_bytes, int32_t use_graph,
+                          mcrt_batch** out) {
+  return guard([&] {
+    if (!out) fail(MCRT_ERR_INVALID, "out is NULL");
+    int c = 0;
+    cuda_check(cudaGetDeviceCount(&c), "cudaGetDeviceCount");
+    if (device < 0 || device >= c) fail(MCRT_ERR_INVALID, "no such CUDA device");
+    if (capacity < 1) fail(MCRT_ERR_INVALID, "capacity must be positive");
+    if (arena_bytes < 4096) fail(MCRT_ERR_INVALID, "memory budget too small");
+    std::unique_ptr<mcrt_batch> b(new mcrt_batch());
+    b->device = device;
+    cuda_check(b->engine.init(device, capacity, static_cast<size_t>(arena_bytes), use_graph != 0), "batch setup");
+    *out = b.release();
+  });
+}
+
+int32_t mcrt_batch_destroy(mcrt_batch* b) {
+  return guard([&] {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    delete b;
+  });
+}
+
+int32_t mcrt_batch_set_chunk(mcrt_batch* b, int32_t paths) {
+  return guard([&] {
+    checked_batch(b);
+    if (paths < 0) fail(MCRT_ERR_INVALID, "negative chunk size");
+    b->engine.set_chunk_paths(paths);
+  });
+}
+
+int32_t mcrt_batch_submit(mcrt_batch* b, const mcrt_request* r, int64_t* id) {
+  return guard([&] {
+    checked_batch(b);
+    const int64_t v = submit_request(b, r);
+    if (id) *id = v;
+  });
+}
+
+int32_t mcrt_batch_cancel(mcrt_batch* b, int64_t id) {
+  return guard([&] {
+    checked_batch(b);
+    b->engine.cancel(id);
+  });
+}
+
+int32_t mcrt_batch_step(mcrt_batch* b, mcrt_batch_event* events, int32_t max_events, int32_t* n_events,
+                        int32_t* idle) {
+  return guard([&] {
+    checked_batch(b);
+    if (max_events < 0 || (max_events > 0 && !events)) fail(MCRT_ERR_INVALID, "bad event buffer");
+    check_slots(b);
+    std::vector<BatchEvent> ev;
+    bool is_idle = false;
+    cuda_check(b->engine.step(ev, &is_idle), "batch step");
+    if (b->engine.totals().status & kStatusIterationLimit)
+      fail(MCRT_ERR_CUDA, "a batched chunk did not finish within its iteration limit");
+    for (const BatchEvent& e : ev) b->pending.push_back(e);
+    int n = 0;
+    while (n < max_events && !b->pending.empty()) {
+      const BatchEvent& e = b->pending.front();
+      events[n++] = mcrt_batch_event{e.id, e.kind, e.samples};
+      b->pending.pop_front();
+    }
+    if (n_events) *n_events = n;
+    if (idle) *idle = is_idle && b->pending.empty() ? 1 : 0;
+  });
+}
+
+int32_t mcrt_batch_render(mcrt_batch* b, int32_t count, const mcrt_request* requests) {
+  return guard([&] {
+    checked_batch(b);
+    if (count < 0 || (count > 0 && !requests)) fail(MCRT_ERR_INVALID, "bad request list");
+    for (int i = 0; i < count; i++) submit_request(b, requests + i);
+    // Every chunk makes progress or the engine is idle, so this loop ends;
+    // the bound only guards against a scheduling fault.
+    bool idle = false;
+    for (long long guard_steps = 0; !idle; guard_steps++) {
+      if (guard_steps > (1LL << 40)) fail(MCRT_ERR_LIMIT, "batch did not finish");
+      check_slots(b);
+      std::vector<BatchEvent> ev;
+      cuda_check(b->engine.step(ev, &idle), "batch step");
+      if (b->engine.totals().status & kStatusIterationLimit)
+        fail(MCRT_ERR_CUDA, "a batched chunk did not finish within its iteration limit");
+    }
+  });
+}
+
+int32_t mcrt_batch_get_stats(mcrt_batch* b, mcrt_batch_stats* out) {
+  return guard([&] {
+    checked_batch(b);
+    if (!out) fail(MCRT_ERR_INVALID, "out is NULL");
+    const BatchTotals t = b->engine.totals();
+    mcrt_batch_stats r{};
+    r.closest_rays = t.closest;
+    r.any_rays = t.any;
+    r.samples = t.samples;
+    r.chunks = t.chunks;
+    r.graph_launches = t.graph_launches;
+    r.gpu_ms = t.gpu_ms;
+    r.arena_bytes = b->engine.arena().capacity();
+    r.arena_used = b->engine.arena().used();
+    r.path_bytes = b->engine.path_bytes();
+    r.status = t.status;
+    *out = r;
   });
 }
 

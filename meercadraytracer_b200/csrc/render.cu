@@ -44,8 +44,9 @@ MCRT_D unsigned int queue_append(unsigned int* counter) {
 
 // ---------------------------------------------------------------- mapping
 MCRT_D void path_pixel(const FrameParams& fp, int pid, int& px, int& py, int& pass) {
-  int j = pid / fp.npix;
-  int i = fp.pix0 + (pid - j * fp.npix);
+  const int k = pid - fp.path_base;
+  int j = k / fp.npix;
+  int i = fp.pix0 + (k - j * fp.npix);
   pass = fp.pass0 + j;
   if (fp.mode == 1) {
     px = fp.list_x[i];
@@ -87,9 +88,7 @@ MCRT_D void unproject(const FrameParams& fp, double x, double y, double z, doubl
 }
 
 // ------------------------------------------------------------------ raygen
-__global__ void __launch_bounds__(kBlock) k_raygen(FrameParams fp, PathState ps, int n) {
-  const int pid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pid >= n) return;
+MCRT_D void raygen_path(const FrameParams& fp, const PathState& ps, int pid) {
   int px, py, pass;
   path_pixel(fp, pid, px, py, pass);
   uint32_t rng;
@@ -112,6 +111,11 @@ __global__ void __launch_bounds__(kBlock) k_raygen(FrameParams fp, PathState ps,
   ps.flags[pid] = kFlagToneMap | kFlagCull;
   ps.smask[pid] = 0ull;
   ps.queue[0][pid] = pid;
+}
+
+__global__ void __launch_bounds__(kBlock) k_raygen(FrameParams fp, PathState ps, int n) {
+  const int pid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pid < n) raygen_path(fp, ps, pid);
 }
 
 // ------------------------------------------------------------------ extend
@@ -178,6 +182,14 @@ MCRT_D bool light_at(const DLight& L, V3 p, V3& l, V3& radiance, float& distance
   return false;
 }
 
+// Where a shade step puts its output: continuing paths and shadow rays.
+struct StageQueues {
+  int* next;
+  unsigned int* next_count;
+  float4* shadow;  // 3 float4 per shadow ray
+  unsigned int* shadow_count;
+};
+
 struct ShadowEmitter {
   float4* queue;
   unsigned int* counter;
@@ -210,12 +222,8 @@ MCRT_D void direct_light(const FrameParams& fp, const DScene& sc, ShadowEmitter&
   em.emit(p + g * side, l, max_t, c * weight, li, fp.shadows == 1);
 }
 
-__global__ void __launch_bounds__(kBlock) k_shade(DScene sc, FrameParams fp, PathState ps,
-                                                  const int* __restrict__ qin, int n, int* __restrict__ qout,
-                                                  Counters* cnt) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n) return;
-  const int pid = qin[q];
+// One iteration of samplePixel's loop for path `pid`.
+MCRT_D void shade_path(const DScene& sc, const FrameParams& fp, const PathState& ps, int pid, const StageQueues& qs) {
   const float4 o4 = ps.ray_o[pid], d4 = ps.ray_d[pid], h4 = ps.hit[pid];
   float4 T4 = ps.thr[pid], L4 = ps.rad[pid];
   uint32_t fl = ps.flags[pid];
@@ -225,7 +233,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(DScene sc, FrameParams fp, Pat
   V3 Lr = V3{L4.x, L4.y, L4.z};
   float fog_factor = T4.w;
   float last_env_scale = L4.w;
-  ShadowEmitter em{ps.shadow_queue, &cnt->shadow_count, pid, 0ull};
+  ShadowEmitter em{qs.shadow, qs.shadow_count, pid, 0ull};
   const unsigned word = __float_as_uint(h4.w);
   const int tri = static_cast<int>(word & 0x7fffffffu) - 1;
   const bool front = (word & 0x80000000u) != 0;
@@ -333,7 +341,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(DScene sc, FrameParams fp, Pat
       const float side = dot(g, d) > 0.0f ? sc.eps : -sc.eps;
       V3 no = p + g * side;
       ps.ray_o[pid] = make_float4(no.x, no.y, no.z, 0.0f);
-      qout[queue_append(&cnt->next_count)] = pid;
+      qs.next[queue_append(qs.next_count)] = pid;
     }
     ps.thr[pid] = make_float4(T.x, T.y, T.z, fog_factor);
     ps.rng[pid] = rng;
@@ -633,7 +641,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(DScene sc, FrameParams fp, Pat
           ps.ray_o[pid] = make_float4(no.x, no.y, no.z, 0.0f);
           ps.ray_d[pid] = make_float4(sdir.x, sdir.y, sdir.z, 0.0f);
           ps.med[pid] = make_float4(med.x, med.y, med.z, 0.0f);
-          qout[queue_append(&cnt->next_count)] = pid;
+          qs.next[queue_append(qs.next_count)] = pid;
         }
       }
     }
@@ -644,6 +652,15 @@ __global__ void __launch_bounds__(kBlock) k_shade(DScene sc, FrameParams fp, Pat
   ps.rng[pid] = rng;
   ps.flags[pid] = fl;
   ps.smask[pid] = em.mask;
+}
+
+__global__ void __launch_bounds__(kBlock) k_shade(DScene sc, FrameParams fp, PathState ps,
+                                                  const int* __restrict__ qin, int n, int* __restrict__ qout,
+                                                  Counters* cnt) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const StageQueues qs{qout, &cnt->next_count, ps.shadow_queue, &cnt->shadow_count};
+  shade_path(sc, fp, ps, qin[q], qs);
 }
 
 // ------------------------------------------------------------------ shadow
@@ -763,11 +780,8 @@ __global__ void __launch_bounds__(kBlock) k_shadow(DScene sc, PathState ps, int 
 }
 
 // ----------------------------------------------------------------- resolve
-__global__ void __launch_bounds__(kBlock) k_resolve(DScene sc, FrameParams fp, PathState ps,
-                                                    const int* __restrict__ queue, int n, int capacity) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n) return;
-  const int pid = queue[q];
+// Adds the path's shadowed light; tone maps and fogs a finished path.
+MCRT_D void resolve_path(const DScene& sc, const FrameParams& fp, const PathState& ps, int pid, int capacity) {
   const uint32_t fl = ps.flags[pid];
   unsigned long long mask = ps.smask[pid];
   if (mask == 0ull && !(fl & kFlagDone)) return;
@@ -796,7 +810,38 @@ __global__ void __launch_bounds__(kBlock) k_resolve(DScene sc, FrameParams fp, P
   ps.sample[pid] = make_float4(c[0], c[1], c[2], 1.0f);
 }
 
+__global__ void __launch_bounds__(kBlock) k_resolve(DScene sc, FrameParams fp, PathState ps,
+                                                    const int* __restrict__ queue, int n, int capacity) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) resolve_path(sc, fp, ps, queue[q], capacity);
+}
+
 // -------------------------------------------------------------- accumulate
+// writeTile's encode, progressive.ts:299-310: average, un-premultiply, sRGB,
+// then the Uint8ClampedArray store.
+MCRT_D uchar4 encode_rgba(double r, double g, double b, double a, double scale, int srgb) {
+  r *= scale;
+  g *= scale;
+  b *= scale;
+  a *= scale;
+  if (a > 0) {
+    r /= a;
+    g /= a;
+    b /= a;
+  }
+  if (srgb) {
+    r = linear_to_srgb_f64(fmax(0.0, r));
+    g = linear_to_srgb_f64(fmax(0.0, g));
+    b = linear_to_srgb_f64(fmax(0.0, b));
+  }
+  uchar4 o;
+  o.x = encode_byte(r);
+  o.y = encode_byte(g);
+  o.z = encode_byte(b);
+  o.w = encode_byte(a);
+  return o;
+}
+
 // writeTile, progressive.ts:295-310, over the passes of one chunk in order.
 // The running sum is Float32; the encode reads the last pass's sum unrounded,
 // as `r = sum[d] = sum[d] + r` does, in double.
@@ -818,26 +863,7 @@ __global__ void __launch_bounds__(256) k_accumulate(const float4* __restrict__ s
   }
   sum[gi] = s;
   if (!last_chunk || !image) return;
-  const double scale = 1.0 / total_passes;
-  r *= scale;
-  g *= scale;
-  b *= scale;
-  a *= scale;
-  if (a > 0) {
-    r /= a;
-    g /= a;
-    b /= a;
-  }
-  if (srgb) {
-    r = linear_to_srgb_f64(fmax(0.0, r));
-    g = linear_to_srgb_f64(fmax(0.0, g));
-    b = linear_to_srgb_f64(fmax(0.0, b));
-  }
-  uchar4 o;
-  o.x = encode_byte(r);
-  o.y = encode_byte(g);
-  o.z = encode_byte(b);
-  o.w = encode_byte(a);
+  const uchar4 o = encode_rgba(r, g, b, a, 1.0 / total_passes, srgb);
   if (fp.mode == 1) {
     reinterpret_cast<uchar4*>(image)[gi] = o;
   } else {
@@ -982,6 +1008,7 @@ cudaError_t PathBuffers::reserve(int capacity, int slots) {
   MCRT_ALLOC(flags, n)
   MCRT_ALLOC(smask, n)
   MCRT_ALLOC(sample, n)
+  MCRT_ALLOC(seg, n)
   MCRT_ALLOC(slots, n * slots)
   MCRT_ALLOC(shadow_queue, n * slots * 3)
 #undef MCRT_ALLOC
@@ -1172,6 +1199,211 @@ cudaError_t launch_count_hits(const DScene& scene, const float4* rays, int count
   if (count <= 0) return cudaSuccess;
   cudaMemsetAsync(fetch, 0, sizeof(unsigned), s);
   k_count_hits<<<persistent_blocks(k_count_hits, count), kBlock, 0, s>>>(scene, rays, count, counts, fetch);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ batched renders
+namespace {
+
+// The segment holding item `k`: the last j < n with base[j] <= k.
+MCRT_D int find_segment(const int* base, int n, int k) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (base[mid] <= k) {
+      lo = mid;
+    } else {
+      hi = mid - 1;
+    }
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kBlock) k_batch_raygen(const BatchTables* __restrict__ t, PathState ps) {
+  __shared__ int base[kMaxSegments + 1];
+  const int nseg = t->segments;
+  for (int i = threadIdx.x; i <= nseg; i += blockDim.x) base[i] = t->seg_base[i];
+  __syncthreads();
+  const int n = t->paths;
+  for (int pid = blockIdx.x * blockDim.x + threadIdx.x; pid < n; pid += gridDim.x * blockDim.x) {
+    const int j = find_segment(base, nseg, pid);
+    ps.seg[pid] = j;
+    raygen_path(t->fp[j], ps, pid);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_batch_extend(DScene sc, int s, BatchTables* t, PathState ps,
+                                                         BatchCounters* bc) {
+  SceneQueues* sq = &t->scenes[s];
+  const int n = static_cast<int>(sq->count);
+  if (n == 0) return;
+  __shared__ int stack_mem[kShort * kBlock];
+  TravStack st;
+  st.smem = stack_mem + threadIdx.x;
+  st.stride = kBlock;
+  st.sp = 0;
+  unsigned status = 0;
+  ExtendQuery q{sc, ps, ps.queue[t->iteration & 1] + sq->base, 0, {}};
+  traverse_persistent(sc, q, n, &sq->fetch, st, status);
+  if (status) atomicOr(&bc->status, status);
+}
+
+__global__ void __launch_bounds__(kBlock) k_batch_shade(DScene sc, int s, BatchTables* t, PathState ps, int slots) {
+  SceneQueues* sq = &t->scenes[s];
+  const int n = static_cast<int>(sq->count);
+  const int cur = t->iteration & 1;
+  const int* qin = ps.queue[cur] + sq->base;
+  const StageQueues qs{ps.queue[cur ^ 1] + sq->base, &sq->next_count,
+                       ps.shadow_queue + 3ull * sq->base * static_cast<unsigned>(slots), &sq->shadow_count};
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int pid = qin[q];
+    shade_path(sc, t->fp[ps.seg[pid]], ps, pid, qs);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_batch_shadow(DScene sc, int s, BatchTables* t, PathState ps, int capacity,
+                                                         int slots, BatchCounters* bc) {
+  SceneQueues* sq = &t->scenes[s];
+  const int n = static_cast<int>(sq->shadow_count);
+  if (n == 0) return;
+  __shared__ int stack_mem[kShort * kBlock];
+  TravStack st;
+  st.smem = stack_mem + threadIdx.x;
+  st.stride = kBlock;
+  st.sp = 0;
+  unsigned status = 0;
+  PathState pq = ps;
+  pq.shadow_queue += 3ull * sq->base * static_cast<unsigned>(slots);
+  ShadowQuery q{sc, pq, capacity, &status};
+  traverse_persistent(sc, q, n, &sq->fetch_shadow, st, status);
+  if (status) atomicOr(&bc->status, status);
+}
+
+__global__ void __launch_bounds__(kBlock) k_batch_resolve(DScene sc, int s, BatchTables* t, PathState ps,
+                                                          int capacity) {
+  SceneQueues* sq = &t->scenes[s];
+  const int n = static_cast<int>(sq->count);
+  const int* qin = ps.queue[t->iteration & 1] + sq->base;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int pid = qin[q];
+    resolve_path(sc, t->fp[ps.seg[pid]], ps, pid, capacity);
+  }
+}
+
+// Queue swap after an iteration, on one thread: counts the queries traced,
+// makes the continued paths the next iteration's queue and says whether
+// another iteration is needed.
+__global__ void k_batch_advance(BatchTables* t, int nscenes, BatchCounters* bc, int graph,
+                                cudaGraphConditionalHandle handle) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  bool more = false;
+  unsigned long long closest = 0, any = 0;
+  for (int s = 0; s < nscenes; s++) {
+    SceneQueues& q = t->scenes[s];
+    closest += q.count;
+    any += q.shadow_count;
+    q.count = q.next_count;
+    q.next_count = 0;
+    q.shadow_count = 0;
+    q.fetch = 0;
+    q.fetch_shadow = 0;
+    more = more || q.count > 0;
+  }
+  bc->closest += closest;
+  bc->any += any;
+  const int it = t->iteration + 1;
+  t->iteration = it;
+  if (more && it >= t->max_iterations) {
+    bc->status |= kStatusIterationLimit;
+    more = false;
+  }
+  bc->more = more ? 1u : 0u;
+  if (graph) cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
+// writeTile for one segment item: a preview block written straight into the
+// image (no running sum, count 1), or one pixel's passes added in order to the
+// Float32 sum and the average encoded.
+__global__ void __launch_bounds__(256) k_batch_accumulate(const BatchTables* __restrict__ t, PathState ps) {
+  __shared__ int base[kMaxSegments + 1];
+  const int nseg = t->segments;
+  for (int i = threadIdx.x; i <= nseg; i += blockDim.x) base[i] = t->pix_base[i];
+  __syncthreads();
+  const int total = base[nseg];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    const int j = find_segment(base, nseg, k);
+    const int i = k - base[j];
+    const FrameParams& fp = t->fp[j];
+    const SegmentOut& o = t->out[j];
+    const float4* samples = ps.sample + t->seg_base[j];
+    uchar4* image = reinterpret_cast<uchar4*>(o.image);
+    if (o.preview) {
+      const float4 x = samples[i];
+      const uchar4 c = encode_rgba(x.x, x.y, x.z, x.w, 1.0, o.srgb);
+      const int bi = fp.pix0 + i;
+      const int by = bi / fp.nbx, bx = bi - by * fp.nbx;
+      const int x0 = fp.tile_x + bx * fp.block, y0 = fp.tile_y + by * fp.block;
+      const int x1 = min(x0 + fp.block, fp.tile_x + fp.tile_w), y1 = min(y0 + fp.block, fp.tile_y + fp.tile_h);
+      for (int y = y0; y < y1; y++)
+        for (int xx = x0; xx < x1; xx++) image[static_cast<size_t>(y) * fp.width + xx] = c;
+      continue;
+    }
+    const int gi = fp.pix0 + i;
+    float4 sm = o.sum[gi];
+    double r = 0, g = 0, b = 0, a = 0;
+    for (int jj = 0; jj < o.passes; jj++) {
+      const float4 x = samples[static_cast<size_t>(jj) * fp.npix + i];
+      r = static_cast<double>(sm.x) + x.x;
+      g = static_cast<double>(sm.y) + x.y;
+      b = static_cast<double>(sm.z) + x.z;
+      a = static_cast<double>(sm.w) + x.w;
+      sm = make_float4(static_cast<float>(r), static_cast<float>(g), static_cast<float>(b), static_cast<float>(a));
+    }
+    o.sum[gi] = sm;
+    const int px = fp.tile_x + gi % fp.tile_w, py = fp.tile_y + gi / fp.tile_w;
+    image[static_cast<size_t>(py) * fp.width + px] = encode_rgba(r, g, b, a, 1.0 / o.done_after, o.srgb);
+  }
+}
+
+int resident_blocks(const void* kernel, int block) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+  return std::max(1, sms * std::max(1, per_sm));
+}
+
+}  // namespace
+
+cudaError_t batch_grids(BatchGrids* g) {
+  g->raygen = resident_blocks(reinterpret_cast<const void*>(k_batch_raygen), kBlock);
+  g->extend = resident_blocks(reinterpret_cast<const void*>(k_batch_extend), kBlock);
+  g->shade = resident_blocks(reinterpret_cast<const void*>(k_batch_shade), kBlock);
+  g->shadow = resident_blocks(reinterpret_cast<const void*>(k_batch_shadow), kBlock);
+  g->resolve = resident_blocks(reinterpret_cast<const void*>(k_batch_resolve), kBlock);
+  g->accumulate = resident_blocks(reinterpret_cast<const void*>(k_batch_accumulate), 256);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_raygen(const BatchTables* t, const PathState& ps, const BatchGrids& g, cudaStream_t s) {
+  k_batch_raygen<<<g.raygen, kBlock, 0, s>>>(t, ps);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_iteration(const DScene* scenes, int nscenes, BatchTables* t, const PathState& ps,
+                                   int capacity, int slots, BatchCounters* counters, const BatchGrids& g, bool graph,
+                                   cudaGraphConditionalHandle handle, cudaStream_t s) {
+  for (int i = 0; i < nscenes; i++) k_batch_extend<<<g.extend, kBlock, 0, s>>>(scenes[i], i, t, ps, counters);
+  for (int i = 0; i < nscenes; i++) k_batch_shade<<<g.shade, kBlock, 0, s>>>(scenes[i], i, t, ps, slots);
+  for (int i = 0; i < nscenes; i++)
+    k_batch_shadow<<<g.shadow, kBlock, 0, s>>>(scenes[i], i, t, ps, capacity, slots, counters);
+  for (int i = 0; i < nscenes; i++) k_batch_resolve<<<g.resolve, kBlock, 0, s>>>(scenes[i], i, t, ps, capacity);
+  k_batch_advance<<<1, 32, 0, s>>>(t, nscenes, counters, graph ? 1 : 0, handle);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_accumulate(const BatchTables* t, const PathState& ps, const BatchGrids& g, cudaStream_t s) {
+  k_batch_accumulate<<<g.accumulate, 256, 0, s>>>(t, ps);
   return cudaGetLastError();
 }
 

@@ -42,6 +42,7 @@ struct FrameParams {
   float clear_color[3], clear_alpha;
   int slot_count;  // shadow slots per path: lights + 1
   int capacity;    // path-state capacity
+  int path_base;   // path id of this launch series' first path (0 unless batched)
 };
 
 // Structure-of-arrays path state, indexed by path id.
@@ -59,6 +60,7 @@ struct PathState {
   float4* slots;   // [slot][capacity] shadow contributions
   int* queue[2];
   float4* shadow_queue;  // 3 float4 per shadow ray
+  int* seg;              // batched renders: the segment each path belongs to
 };
 
 struct Counters {
@@ -117,6 +119,79 @@ class Wavefront {
 // Camera rays of one pass over fp.npix paths and their closest hits, left in
 // the path state's `hit` array.
 cudaError_t primary_hits(const DScene& scene, FrameParams fp, PathBuffers& buffers, cudaStream_t stream);
+
+// ----------------------------------------------------------- batched renders
+// Many requests (cameras, scenes, sizes, sample counts) share one path pool.
+// A chunk is a list of segments, each one request's passes [pass0, pass0 +
+// passes) over its pixels (or preview blocks) [pix0, pix0 + npix), at most one
+// segment per request, grouped by scene: the paths of scene s hold the ids
+// [base, base + paths), and its queue entries and shadow rays use the
+// matching ranges of the queues, so every stage runs once per scene.
+constexpr int kMaxBatchScenes = 8;
+constexpr int kMaxSegments = 256;
+constexpr unsigned kStatusIterationLimit = 16u;  // a chunk still had paths after max_iterations
+
+struct SceneQueues {
+  unsigned base;          // first path id of the scene in this chunk
+  unsigned paths;
+  unsigned count;         // paths queued for this iteration's closest hits
+  unsigned next_count;    // paths this iteration's shade step continued
+  unsigned shadow_count;  // shadow rays of this iteration
+  unsigned fetch;         // work counters of the persistent traversals
+  unsigned fetch_shadow;
+  unsigned pad;
+};
+
+// Where a segment's samples go.
+struct SegmentOut {
+  float4* sum;      // the request's Float32 running sums, one per pixel
+  uint8_t* image;   // the request's RGBA8 image
+  int passes;       // passes in this segment
+  int done_after;   // passes accumulated once this segment is in
+  int preview;      // a block preview: written straight into the image
+  int srgb;
+};
+
+// Everything a chunk's kernels read, uploaded once per chunk.
+struct BatchTables {
+  int segments;
+  int paths;
+  int iteration;       // wavefront iteration (queue parity)
+  int max_iterations;
+  int seg_base[kMaxSegments + 1];  // first path of each segment; [segments] = paths
+  int pix_base[kMaxSegments + 1];  // first accumulate item of each segment; [segments] = total
+  SceneQueues scenes[kMaxBatchScenes];
+  SegmentOut out[kMaxSegments];
+  FrameParams fp[kMaxSegments];    // per segment; path_base = seg_base[j]
+};
+
+// Device totals that outlive the per-chunk uploads.
+struct BatchCounters {
+  unsigned long long closest;  // closest-hit queries traced
+  unsigned long long any;      // shadow queries traced
+  unsigned long long samples;
+  unsigned status;
+  unsigned more;               // set by the iteration step when paths remain (host-driven loop)
+};
+
+// Grid sizes of the batched kernels on the current device.
+struct BatchGrids {
+  int raygen, extend, shade, shadow, resolve, accumulate;
+};
+
+cudaError_t batch_grids(BatchGrids* g);
+// Camera rays of every segment of the chunk.
+cudaError_t launch_batch_raygen(const BatchTables* t, const PathState& ps, const BatchGrids& g, cudaStream_t s);
+// One wavefront iteration over every scene: closest hits, shading, shadow
+// rays, resolve, then the queue swap. `graph`: the swap sets conditional
+// `handle` (the loop runs as a graph's while node); otherwise it sets
+// counters->more for a host-driven loop.
+cudaError_t launch_batch_iteration(const DScene* scenes, int nscenes, BatchTables* t, const PathState& ps,
+                                   int capacity, int slots, BatchCounters* counters, const BatchGrids& g, bool graph,
+                                   cudaGraphConditionalHandle handle, cudaStream_t s);
+// Accumulates (or, for previews, writes) every segment's samples and encodes
+// the requests' images.
+cudaError_t launch_batch_accumulate(const BatchTables* t, const PathState& ps, const BatchGrids& g, cudaStream_t s);
 
 // Kernel launchers used by the executor.
 cudaError_t launch_accumulate(const float4* samples, int npix, int passes_in_chunk, float4* sum, int total_passes,

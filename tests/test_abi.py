@@ -54,6 +54,8 @@ STRUCTS = {
     "mcrt_light": abi.mcrt_light, "mcrt_fog": abi.mcrt_fog, "mcrt_background": abi.mcrt_background,
     "mcrt_geometry": abi.mcrt_geometry, "mcrt_shading": abi.mcrt_shading, "mcrt_camera": abi.mcrt_camera,
     "mcrt_settings": abi.mcrt_settings, "mcrt_tile": abi.mcrt_tile, "mcrt_stats": mcrt_stats,
+    "mcrt_request": abi.mcrt_request, "mcrt_batch_event": abi.mcrt_batch_event,
+    "mcrt_batch_stats": abi.mcrt_batch_stats,
 }
 
 
