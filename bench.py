@@ -352,10 +352,145 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                                 "sample": f"{base['pixels']} random pixels x {spp} passes ({base['rays']} rays, "
                                           f"{base['seconds']:.1f} s) of the same workload on the oracle, a C++ "
                                           f"restatement of the reference's TypeScript path (no Node.js here)"}
+    if world == 1 and not (args.no_batch and args.no_serve):
+        # The batched and served forms of the same path, beside the plain number.
+        from meercadraytracer_b200 import scenes as SC
+        from meercadraytracer_b200.compile import compile_scene as _compile
+
+        small = SC.small_scene()
+        extra = {"mid": compiled, "small": _compile(small.scene, builder=ex.compile_sink)}
+        if not args.no_batch:
+            line["batched"] = run_batched(extra, local, args.batch_capacity)
+        if not args.no_serve:
+            t0 = time.perf_counter()
+            big = SC.mid_scene(seed=SC.SEED_BASE + 13, grid=32, width=1280, height=720)
+            extra["big"] = _compile(big.scene, builder=ex.compile_sink)
+            extra["soup"] = _compile(SC.soup_scene().scene, builder=ex.compile_sink)
+            t_scenes = time.perf_counter() - t0
+            line["served"] = run_served(extra, local, args.serve_seconds, args.serve_capacity, args.serve_chunk)
+            line["served"]["scene_build_s"] = round(t_scenes, 2)
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
     ex.dispose()
+
+
+# ------------------------------------------------------------ batched renders
+BATCH_RESOLUTIONS = ((256, 256), (512, 512), (640, 480), (1024, 1024))
+BATCH_SPP = (4, 16, 64)
+
+
+def batch_plan(seed: int, count: int = 64) -> List[Tuple[str, Tuple[float, float, float], Tuple[int, int], int]]:
+    """The batched workload: `count` requests over the mid and small scenes (50/50), each with
+    a camera on a sphere of radius U(10, 30) aimed at the origin, a resolution drawn from
+    BATCH_RESOLUTIONS and a sample count from BATCH_SPP."""
+    rng = np.random.default_rng(seed)
+    plan = []
+    for _ in range(count):
+        scene = "mid" if rng.uniform() < 0.5 else "small"
+        d = rng.normal(size=3)
+        d /= max(float(np.linalg.norm(d)), 1e-12)
+        pos = tuple(float(v) for v in d * rng.uniform(10.0, 30.0))
+        res = BATCH_RESOLUTIONS[int(rng.integers(len(BATCH_RESOLUTIONS)))]
+        spp = BATCH_SPP[int(rng.integers(len(BATCH_SPP)))]
+        plan.append((scene, pos, res, spp))
+    return plan
+
+
+def run_batched(compiled: Dict[str, Any], device: int, capacity: int, seed: int = 0x5EED0002) -> Dict[str, Any]:
+    """64 requests rendered one by one through the plain path (mcrt_raytrace per request),
+    then all together through the batch engine (one wavefront, CUDA-graph bounce loop).
+    Both read every image back to the host; the batch's images must equal the plain ones."""
+    from meercadraytracer_b200 import scene as S
+    from meercadraytracer_b200.batch import BatchRenderer, RenderRequest
+    from meercadraytracer_b200.compile import compile_camera
+    from meercadraytracer_b200.executors import GpuExecutor
+    from meercadraytracer_b200.raytrace import trace_settings
+
+    settings = trace_settings({"global_illumination": True, "max_bounces": 4, "tone_mapping": S.ACESFilmicToneMapping})
+    reqs = []
+    for scene, pos, (w, h), spp in batch_plan(seed):
+        cam = S.PerspectiveCamera(50, w / h, 0.1, 2000)
+        cam.position.set(*pos)
+        cam.look_at(0, 0, 0)
+        cam.update_matrix_world()
+        reqs.append(RenderRequest(compiled[scene], compile_camera(cam), w, h, settings, spp))
+    renderer = BatchRenderer(device, capacity, memory_budget=4 << 30)
+    try:
+        # Plain: one raytraceCompiled per request, on executors that already hold the scenes.
+        plain_imgs = []
+        execs = {id(c): renderer.executor(c) for c in compiled.values()}
+        for ex in execs.values():
+            ex.reset_stats()
+            ex.set_capacity(capacity)
+        for r in reqs[:2]:  # warm-up
+            execs[id(r.scene)].raytrace(r.scene, r.camera, r.width, r.height, r.settings, 1, True)
+        for ex in execs.values():
+            ex.reset_stats()
+        t0 = time.perf_counter()
+        for r in reqs:
+            plain_imgs.append(execs[id(r.scene)].raytrace(r.scene, r.camera, r.width, r.height, r.settings,
+                                                           r.samples, True))
+        plain_wall = time.perf_counter() - t0
+        pst = [ex.stats() for ex in execs.values()]
+        plain_rays = sum(x["closest_rays"] + x["any_rays"] for x in pst)
+        plain_ms = sum(x["ms_total"] for x in pst)
+        # Batched: the same requests in one batch.
+        renderer.render(reqs[:2])  # warm-up (graph instantiation)
+        st0 = renderer.stats()
+        t0 = time.perf_counter()
+        imgs = renderer.render(reqs)
+        batch_wall = time.perf_counter() - t0
+        st1 = renderer.stats()
+        rays = (st1["closest_rays"] - st0["closest_rays"]) + (st1["any_rays"] - st0["any_rays"])
+        gpu_ms = st1["gpu_ms"] - st0["gpu_ms"]
+        same = sum(int(np.array_equal(a, b)) for a, b in zip(imgs, plain_imgs))
+        return {
+            "workload": "64 requests, mid (1,310,720 tris) / small (22,530 tris) scenes 50/50, cameras on a sphere "
+                        "of radius U(10,30) aimed at the origin, resolutions {256^2, 512^2, 640x480, 1024^2}, "
+                        "spp {4, 16, 64}, GI on, 4 bounces; images read back to the host",
+            "requests": len(reqs), "samples": int(sum(r.width * r.height * r.samples for r in reqs)),
+            "rays": int(rays), "plain_rays": int(plain_rays),
+            "plain_mrays_s": round(plain_rays / plain_wall / 1e6, 1),
+            "plain_device_mrays_s": round(plain_rays / (plain_ms / 1e3) / 1e6, 1),
+            "batched_mrays_s": round(rays / batch_wall / 1e6, 1),
+            "batched_device_mrays_s": round(rays / (gpu_ms / 1e3) / 1e6, 1),
+            "speedup_vs_plain": round((rays / batch_wall) / (plain_rays / plain_wall), 3),
+            "plain_wall_s": round(plain_wall, 3), "batched_wall_s": round(batch_wall, 3),
+            "chunks": int(st1["chunks"] - st0["chunks"]), "graph_launches": int(st1["graph_launches"] - st0["graph_launches"]),
+            "capacity": capacity, "images_equal_to_plain": f"{same}/{len(reqs)}",
+        }
+    finally:
+        renderer.dispose()
+
+
+# ------------------------------------------------------------- serving loop
+def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: int, chunk: int) -> Dict[str, Any]:
+    """The serving loop: 8 clients, two per resident scene, orbiting at 30 deg/s with Poisson
+    camera moves (mean 100 ms); each move restarts the client's request: an 8x8 block preview,
+    then 64 spp at 1280x720, GI on, 4 bounces. After `seconds` the moves stop and each
+    client's last request runs to 64 spp."""
+    from meercadraytracer_b200 import scene as S
+    from meercadraytracer_b200.raytrace import trace_settings
+    from meercadraytracer_b200.serve import Client, RenderServer, simulate_clients
+
+    settings = trace_settings({"global_illumination": True, "max_bounces": 4, "tone_mapping": S.ACESFilmicToneMapping})
+    orbits = {"small": (17.0, 6.0), "mid": (70.0, 32.0), "big": (130.0, 60.0), "soup": (34.0, 12.0)}
+    names = [n for n in ("small", "mid", "big", "soup") if n in compiled]
+    clients = [Client(names[i % len(names)], *orbits[names[i % len(names)]], phase=45.0 * i) for i in range(8)]
+    server = RenderServer(device, capacity=capacity, memory_budget=2 << 30, chunk_paths=chunk)
+    try:
+        for n in names:
+            server.add_scene(n, compiled[n])
+        # Warm-up: one short request per scene (graph instantiation, first-touch).
+        simulate_clients(server, clients[: len(names)], {n: settings for n in names}, duration=0.2, width=320,
+                         height=180, samples=2, seed=1)
+        out = simulate_clients(server, clients, {n: settings for n in names}, duration=seconds)
+        out["scenes"] = {n: int(compiled[n].geometry.triangle_count) for n in names}
+        out["capacity"], out["chunk_paths"] = capacity, chunk
+        return out
+    finally:
+        server.close()
 
 
 def traffic_from_profile(kernel: str) -> Optional[float]:
@@ -384,6 +519,12 @@ def main() -> None:
     ap.add_argument("--width", type=int, default=0, help="override the image width (profiling runs)")
     ap.add_argument("--height", type=int, default=0, help="override the image height (profiling runs)")
     ap.add_argument("--spp", type=int, default=0, help="override samples per pixel (profiling runs)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-renders comparison")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop run")
+    ap.add_argument("--batch-capacity", type=int, default=1 << 24, help="path pool of the batch engine")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the served client simulation")
+    ap.add_argument("--serve-capacity", type=int, default=1 << 22, help="path pool of the serving loop")
+    ap.add_argument("--serve-chunk", type=int, default=0, help="paths per chunk in the serving loop (0: pool)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be at least 3")

@@ -171,6 +171,17 @@ int32_t mcrt_set_timing(mcrt_executor* executor, int32_t enabled);
 /* Path-state capacity (paths in flight per launch); the autotuner sets it. */
 int32_t mcrt_set_capacity(mcrt_executor* executor, int32_t paths);
 
+/* The traversal kernel variants compiled into the library: up to `max`
+ * (threads per block, shared-memory short-stack entries per thread) pairs,
+ * and *count = how many there are. Variant 0, (128, 16), is the default. No
+ * counterpart in the reference (its traversal is one JavaScript loop). */
+int32_t mcrt_traversal_variants(int32_t max, int32_t* blocks, int32_t* stacks, int32_t* count);
+
+/* Chooses the closest-hit and shadow traversal kernels of an executor by
+ * block size and short-stack depth (one of mcrt_traversal_variants); the
+ * autotuner sets it. Results do not depend on the choice. */
+int32_t mcrt_set_traversal(mcrt_executor* executor, int32_t block, int32_t stack);
+
 int32_t mcrt_get_stats(mcrt_executor* executor, mcrt_stats* out);
 int32_t mcrt_reset_stats(mcrt_executor* executor);
 
@@ -198,9 +209,14 @@ typedef struct mcrt_request {
   int32_t srgb;             /* encode sRGB output */
   uint8_t* image;           /* host RGBA8, width * height * 4, for the final image; or NULL */
   uint8_t* preview_image;   /* host RGBA8 for the block preview; or NULL */
+  uint8_t* progress_image;  /* host RGBA8 refreshed after every chunk that completes a pass short of the
+                               last (ProgressiveFrame with samples < maxSamples); or NULL */
 } mcrt_request;
 
-enum { MCRT_EVENT_PREVIEW = 1, MCRT_EVENT_DONE = 2 };
+/* PREVIEW: preview_image holds the block preview. PROGRESS: `samples` passes
+ * are accumulated (progress_image holds them, if given). DONE: image holds
+ * the final image. */
+enum { MCRT_EVENT_PREVIEW = 1, MCRT_EVENT_DONE = 2, MCRT_EVENT_PROGRESS = 3 };
 
 typedef struct mcrt_batch_event {
   int64_t id;
@@ -227,6 +243,8 @@ int32_t mcrt_batch_create(int32_t device, int32_t capacity, int64_t arena_bytes,
 int32_t mcrt_batch_destroy(mcrt_batch* batch);
 /* Paths per chunk (<= capacity); smaller chunks bound preview latency. */
 int32_t mcrt_batch_set_chunk(mcrt_batch* batch, int32_t paths);
+/* As mcrt_set_traversal, for the batch's kernels. */
+int32_t mcrt_batch_set_traversal(mcrt_batch* batch, int32_t block, int32_t stack);
 /* Queues a request; *id identifies it in events. */
 int32_t mcrt_batch_submit(mcrt_batch* batch, const mcrt_request* request, int64_t* id);
 /* Stops a request (a camera move restarts it as a new request). */

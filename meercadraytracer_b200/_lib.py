@@ -85,6 +85,9 @@ SIGNATURES = {
                                      _P(_i32), _P(_u32), _P(_i32), _P(_d), _P(_i32)]),
     "mcrt_set_timing": (_i32, [_vp, _i32]),
     "mcrt_set_capacity": (_i32, [_vp, _i32]),
+    "mcrt_traversal_variants": (_i32, [_i32, _P(_i32), _P(_i32), _P(_i32)]),
+    "mcrt_set_traversal": (_i32, [_vp, _i32, _i32]),
+    "mcrt_batch_set_traversal": (_i32, [_vp, _i32, _i32]),
     "mcrt_get_stats": (_i32, [_vp, _P(mcrt_stats)]),
     "mcrt_reset_stats": (_i32, [_vp]),
 }
@@ -114,3 +117,13 @@ def call(name: str, *args) -> None:
     code = getattr(lib, name)(*args)
     if code != MCRT_OK:
         raise McrtError(code, lib.mcrt_last_error().decode(errors="replace") or f"{name} failed ({code})")
+
+
+def traversal_variants() -> list:
+    """The (threads per block, short-stack entries) pairs the traversal kernels were compiled for."""
+    n = C.c_int32()
+    call("mcrt_traversal_variants", 0, None, None, C.byref(n))
+    blocks = (C.c_int32 * max(1, n.value))()
+    stacks = (C.c_int32 * max(1, n.value))()
+    call("mcrt_traversal_variants", n.value, blocks, stacks, C.byref(n))
+    return [(int(blocks[i]), int(stacks[i])) for i in range(n.value)]

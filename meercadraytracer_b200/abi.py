@@ -135,6 +135,7 @@ class mcrt_request(C.Structure):
         ("camera", mcrt_camera), ("settings", mcrt_settings), ("width", C.c_int32), ("height", C.c_int32),
         ("samples", C.c_int32), ("preview_block", C.c_int32), ("srgb", C.c_int32),
         ("image", C.POINTER(C.c_uint8)), ("preview_image", C.POINTER(C.c_uint8)),
+        ("progress_image", C.POINTER(C.c_uint8)),
     ]
 
 

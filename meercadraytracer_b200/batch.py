@@ -9,8 +9,8 @@ cameras, sizes and sample counts) together in one wavefront on one GPU:
     renderer = BatchRenderer(capacity=1 << 22, memory_budget=4 << 30)
     images = renderer.render([RenderRequest(scene, camera, 512, 512, settings, 16), ...])
 
-or, as a serving loop, submit() / step() / cancel() with preview and done
-events. Each request's final image equals raytrace_compiled's for the same
+or, as a serving loop, submit() / step() / cancel() with preview, progress
+and done events. Each request's final image equals raytrace_compiled's for the same
 inputs, alone or in any mix. Scenes stay resident: each distinct
 CompiledScene is uploaded once, to its own GpuExecutor.
 """
@@ -29,6 +29,7 @@ from .types import CompiledCamera, CompiledScene, TraceSettings
 
 EVENT_PREVIEW = 1
 EVENT_DONE = 2
+EVENT_PROGRESS = 3
 
 
 @dataclass
@@ -43,6 +44,7 @@ class RenderRequest:
     samples: int = 16
     preview_block: int = 0  # > 1: ProgressiveOptions.previewBlock
     srgb: bool = True
+    progress: bool = False  # copy the image to the host after every completed pass
 
 
 class BatchRenderer:
@@ -56,8 +58,9 @@ class BatchRenderer:
              C.byref(handle))
         self._h = handle
         self.device = device
+        self.capacity = int(capacity)
         self._executors: Dict[int, Tuple[CompiledScene, GpuExecutor]] = {}
-        self._buffers: Dict[int, Tuple[np.ndarray, Optional[np.ndarray]]] = {}
+        self._buffers: Dict[int, Tuple[np.ndarray, Optional[np.ndarray], Optional[np.ndarray]]] = {}
 
     # ----------------------------------------------------------- scenes
     def executor(self, scene: CompiledScene) -> GpuExecutor:
@@ -71,32 +74,57 @@ class BatchRenderer:
         return entry[1]
 
     # ---------------------------------------------------------- requests
-    def _c_request(self, r: RenderRequest, image: np.ndarray, preview: Optional[np.ndarray]) -> abi.mcrt_request:
-        ex = self.executor(r.scene)
-        gv, sv = ex.load_scene(r.scene)
+    @staticmethod
+    def _c_fields(ex: GpuExecutor, versions: Tuple[int, int], camera: CompiledCamera, settings: TraceSettings,
+                  width: int, height: int, samples: int, preview_block: int, srgb: bool, image: np.ndarray,
+                  preview: Optional[np.ndarray], progress: Optional[np.ndarray]) -> abi.mcrt_request:
         c = abi.mcrt_request()
         c.scene = ex._h.value
-        c.geometry_version = gv
-        c.shading_version = sv
-        c.camera = abi.to_c_camera(r.camera)
-        c.settings = abi.to_c_settings(r.settings)
-        c.width, c.height = int(r.width), int(r.height)
-        c.samples = int(r.samples)
-        c.preview_block = int(r.preview_block)
-        c.srgb = int(bool(r.srgb))
+        c.geometry_version, c.shading_version = int(versions[0]), int(versions[1])
+        c.camera = abi.to_c_camera(camera)
+        c.settings = abi.to_c_settings(settings)
+        c.width, c.height = int(width), int(height)
+        c.samples = int(samples)
+        c.preview_block = int(preview_block)
+        c.srgb = int(bool(srgb))
+        none = C.cast(None, C.POINTER(C.c_uint8))
         c.image = abi.ptr(image, C.c_uint8)
-        c.preview_image = abi.ptr(preview, C.c_uint8) if preview is not None else C.cast(None, C.POINTER(C.c_uint8))
+        c.preview_image = abi.ptr(preview, C.c_uint8) if preview is not None else none
+        c.progress_image = abi.ptr(progress, C.c_uint8) if progress is not None else none
         return c
 
-    def submit(self, r: RenderRequest) -> int:
-        """Queues a request; returns its id. Its images are result(id) / preview(id)."""
-        image = np.zeros(r.width * r.height * 4, np.uint8)
-        preview = np.zeros(r.width * r.height * 4, np.uint8) if r.preview_block > 1 else None
-        c = self._c_request(r, image, preview)
+    def _c_request(self, r: RenderRequest, image: np.ndarray, preview: Optional[np.ndarray],
+                   progress: Optional[np.ndarray] = None) -> abi.mcrt_request:
+        ex = self.executor(r.scene)
+        versions = ex.load_scene(r.scene)
+        return self._c_fields(ex, versions, r.camera, r.settings, r.width, r.height, r.samples, r.preview_block,
+                              r.srgb, image, preview, progress)
+
+    def _submit_c(self, c: abi.mcrt_request, buffers: Tuple[np.ndarray, Optional[np.ndarray], Optional[np.ndarray]]
+                  ) -> int:
         rid = C.c_int64()
         call("mcrt_batch_submit", self._h, C.byref(c), C.byref(rid))
-        self._buffers[rid.value] = (image, preview)
+        self._buffers[rid.value] = buffers
         return rid.value
+
+    def submit(self, r: RenderRequest) -> int:
+        """Queues a request; returns its id. Its images are result(id) / preview(id) / progress(id)."""
+        image = np.zeros(r.width * r.height * 4, np.uint8)
+        preview = np.zeros(r.width * r.height * 4, np.uint8) if r.preview_block > 1 else None
+        progress = np.zeros(r.width * r.height * 4, np.uint8) if r.progress else None
+        return self._submit_c(self._c_request(r, image, preview, progress), (image, preview, progress))
+
+    def submit_to(self, executor: GpuExecutor, versions: Tuple[int, int], camera: CompiledCamera,
+                  settings: TraceSettings, width: int, height: int, samples: int, preview_block: int = 0,
+                  srgb: bool = True, progress: bool = False) -> int:
+        """As submit, for a scene that `executor` already holds under `versions` (geometry, shading),
+        as SceneSync.sync leaves it."""
+        image = np.zeros(width * height * 4, np.uint8)
+        preview = np.zeros(width * height * 4, np.uint8) if preview_block > 1 else None
+        prog = np.zeros(width * height * 4, np.uint8) if progress else None
+        c = self._c_fields(executor, versions, camera, settings, width, height, samples, preview_block, srgb, image,
+                           preview, prog)
+        return self._submit_c(c, (image, preview, prog))
 
     def cancel(self, rid: int) -> None:
         call("mcrt_batch_cancel", self._h, int(rid))
@@ -115,6 +143,10 @@ class BatchRenderer:
     def preview(self, rid: int) -> Optional[np.ndarray]:
         return self._buffers[rid][1]
 
+    def progress(self, rid: int) -> Optional[np.ndarray]:
+        """The image after the last completed pass (requests submitted with progress=True)."""
+        return self._buffers[rid][2]
+
     def forget(self, rid: int) -> None:
         """Drops the host buffers of a finished or cancelled request."""
         self._buffers.pop(rid, None)
@@ -130,6 +162,10 @@ class BatchRenderer:
 
     def set_chunk(self, paths: int) -> None:
         call("mcrt_batch_set_chunk", self._h, int(paths))
+
+    def set_traversal(self, block: int, stack: int) -> None:
+        """Traversal kernels by threads per block and short-stack depth (_lib.traversal_variants())."""
+        call("mcrt_batch_set_traversal", self._h, int(block), int(stack))
 
     def stats(self) -> Dict[str, float]:
         s = abi.mcrt_batch_stats()

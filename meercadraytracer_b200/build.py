@@ -14,6 +14,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from typing import List
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -56,17 +57,24 @@ def build(force: bool = False, verbose: bool = False, extra: List[str] = ()) -> 
     headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "mcrt.h"),
                                                           os.path.join(ROOT, "include", "mcrt_types.h")]
     objects = []
-    changed = force
+    commands = []
     for src, flags in SOURCES.items():
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
         objects.append(obj)
         if force or _stale(obj, [path, *headers]):
-            cmd = [nvcc(), *common_flags(), *flags, *extra, "-c", path, "-o", obj]
+            commands.append([nvcc(), *common_flags(), *flags, *extra, "-c", path, "-o", obj])
+    changed = force or bool(commands)
+    # The translation units are independent: compile them side by side.
+    with ThreadPoolExecutor(max_workers=max(1, min(len(commands), os.cpu_count() or 1))) as pool:
+        for cmd in commands:
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
-            changed = True
+        for r in list(pool.map(lambda c: subprocess.run(c, capture_output=not verbose, text=True), commands)):
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed: {' '.join(r.args)}\n{r.stdout or ''}{r.stderr or ''}")
+            if extra and r.stderr:
+                print(r.stderr, flush=True)
     if changed or _stale(LIB, objects):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objects, "-lcudart"]
         if verbose:

@@ -323,9 +323,33 @@ def _normal_matrix(m: np.ndarray) -> Tuple[np.ndarray, float]:
     return n, det
 
 
+def js_hypot_rows(v: np.ndarray) -> np.ndarray:
+    """Math.hypot(x, y, z) of each row as V8 computes it: the values scaled by the
+    largest magnitude, their squares summed with Kahan compensation, then
+    sqrt(sum) * largest. Rows with an infinity give infinity, rows with a NaN NaN."""
+    a = np.abs(v)
+    mx = a.max(axis=1)
+    safe = np.where(mx > 0, mx, 1.0)
+    total = np.zeros(v.shape[0])
+    comp = np.zeros(v.shape[0])
+    with np.errstate(invalid="ignore", over="ignore"):
+        for k in range(3):
+            n = a[:, k] / safe
+            summand = n * n - comp
+            prelim = total + summand
+            comp = (prelim - total) - summand
+            total = prelim
+        out = np.sqrt(total) * mx
+    out = np.where(mx == 0, 0.0, out)
+    out = np.where(np.isnan(a).any(axis=1), np.nan, out)
+    return np.where(np.isinf(a).any(axis=1), np.inf, out)
+
+
 def _normalise_rows(v: np.ndarray) -> np.ndarray:
-    length = np.sqrt(np.einsum("ij,ij->i", v, v))
-    length = np.where(length > 0, length, 1.0)
+    """`Math.hypot(nx, ny, nz) || 1` and the divisions of addMesh (src/compile.ts:268-270)."""
+    length = js_hypot_rows(v)
+    length = np.where((length > 0) | np.isnan(length), length, 1.0)
+    length = np.where(np.isnan(length), 1.0, length)
     return v / length[:, None]
 
 
@@ -397,8 +421,11 @@ def flatten_meshes(meshes: Sequence[S.Mesh], material_index: Callable[[Any], int
                 else:
                     e = p[:, 3:6] - p[:, 0:3]
                     f = p[:, 6:9] - p[:, 0:3]
-                    face = np.cross(e, f)
-                    length = np.sqrt(np.einsum("ij,ij->i", face, face))
+                    # normalize(), src/compile.ts:52-55, of the cross product written out as
+                    # compile.ts:287-289 does.
+                    face = np.stack([e[:, 1] * f[:, 2] - e[:, 2] * f[:, 1], e[:, 2] * f[:, 0] - e[:, 0] * f[:, 2],
+                                     e[:, 0] * f[:, 1] - e[:, 1] * f[:, 0]], axis=1)
+                    length = js_hypot_rows(face)
                     face = np.where(length[:, None] > 0, face / np.where(length > 0, length, 1)[:, None],
                                     np.array([0.0, 0.0, 1.0]))
                     n = np.tile(face, (1, 3))

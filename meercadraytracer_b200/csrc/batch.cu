@@ -77,6 +77,7 @@ BatchEngine::~BatchEngine() {
     if (c.done) cudaEventDestroy(c.done);
     if (c.copied) cudaEventDestroy(c.copied);
   }
+  if (last_copy_) cudaEventDestroy(last_copy_);
   destroy_graph();
   if (tables_dev_) cudaFree(tables_dev_);
   for (BatchTables* t : tables_host_)
@@ -94,6 +95,7 @@ cudaError_t BatchEngine::init(int device, int capacity, size_t arena_bytes, bool
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&last_copy_, cudaEventDisableTiming);
   if (e == cudaSuccess) e = arena_.init(arena_bytes);
   if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&tables_dev_), sizeof(BatchTables));
   for (int i = 0; i < 2 && e == cudaSuccess; i++)
@@ -134,6 +136,15 @@ cudaError_t BatchEngine::set_scene(int slot, const DScene& scene, int lights) {
   slots_ = std::max(slots_, slots);
   graph_valid_ = false;
   return cudaSuccess;
+}
+
+cudaError_t BatchEngine::set_variant(int variant) {
+  if (variant == grids_.variant) return cudaSuccess;
+  cudaSetDevice(device_);
+  cudaError_t e = cudaStreamSynchronize(stream_);
+  if (e == cudaSuccess) e = batch_grids(&grids_, variant);
+  graph_valid_ = false;
+  return e;
 }
 
 void BatchEngine::destroy_graph() {
@@ -192,7 +203,8 @@ cudaError_t BatchEngine::ensure_graph() {
   return e;
 }
 
-long long BatchEngine::submit(const BatchRequestDesc& d, uint8_t* host_image, uint8_t* host_preview) {
+long long BatchEngine::submit(const BatchRequestDesc& d, uint8_t* host_image, uint8_t* host_preview,
+                              uint8_t* host_progress) {
   if (d.scene < 0 || d.scene >= kMaxBatchScenes || !scene_set_[d.scene]) return -1;
   if (d.fp.width <= 0 || d.fp.height <= 0 || d.samples < 1) return -1;
   auto r = std::make_unique<Request>();
@@ -200,6 +212,7 @@ long long BatchEngine::submit(const BatchRequestDesc& d, uint8_t* host_image, ui
   r->d = d;
   r->host_image = host_image;
   r->host_preview = host_preview;
+  r->host_progress = host_progress;
   r->preview = d.preview_block > 1 ? 1 : 0;
   const long long id = r->id;
   requests_.push_back(std::move(r));
@@ -350,6 +363,11 @@ cudaError_t BatchEngine::launch(Chunk& c) {
   if (e == cudaSuccess) e = ensure_graph();
   if (e == cudaSuccess) e = cudaEventRecord(c.start, stream_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(tables_dev_, T, bytes, cudaMemcpyHostToDevice, stream_);
+  // An image of this chunk's requests may still be on its way to the host
+  // from the chunk before: the kernels below rewrite it, so wait for the copy.
+  bool wait_copy = false;
+  for (const SegmentPlan& s : c.segs) wait_copy = wait_copy || s.r->copying > 0;
+  if (e == cudaSuccess && wait_copy && copy_pending_) e = cudaStreamWaitEvent(stream_, last_copy_, 0);
   if (e != cudaSuccess) return e;
   const PathState ps = paths_.state();
   if (use_graph_) {
@@ -370,19 +388,27 @@ cudaError_t BatchEngine::launch(Chunk& c) {
   if (e == cudaSuccess) e = cudaEventRecord(c.done, stream_);
   if (e != cudaSuccess) return e;
   totals_.chunks++;
-  // Images a request's client is waiting for: its preview, and the final image.
+  // Images a request's client is waiting for: its preview, the image after
+  // each completed pass (when asked for), and the final image.
   c.copies = false;
-  for (const SegmentPlan& s : c.segs) {
-    const Request& r = *s.r;
-    const bool last = !s.preview && s.pass0 + s.passes == r.d.samples && s.pix0 + s.npix == r.pixels();
-    uint8_t* dst = s.preview ? r.host_preview : (last ? r.host_image : nullptr);
+  c.passes_done.assign(c.segs.size(), 0);
+  for (size_t j = 0; j < c.segs.size(); j++) {
+    const SegmentPlan& s = c.segs[j];
+    Request& r = *s.r;
+    const bool pass_end = !s.preview && s.pix0 + s.npix == r.pixels();
+    const bool last = pass_end && s.pass0 + s.passes == r.d.samples;
+    if (pass_end) c.passes_done[j] = s.pass0 + s.passes;
+    uint8_t* dst = s.preview ? r.host_preview : (last ? r.host_image : (pass_end ? r.host_progress : nullptr));
     if (!dst) continue;
     if (!c.copies) e = cudaStreamWaitEvent(copy_stream_, c.done, 0);
     c.copies = true;
+    r.copying++;
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(dst, r.image, static_cast<size_t>(r.pixels()) * 4, cudaMemcpyDeviceToHost, copy_stream_);
   }
   if (e == cudaSuccess && c.copies) e = cudaEventRecord(c.copied, copy_stream_);
+  if (e == cudaSuccess && c.copies) e = cudaEventRecord(last_copy_, copy_stream_);
+  if (c.copies) copy_pending_ = true;
   return e;
 }
 
@@ -397,17 +423,25 @@ cudaError_t BatchEngine::finish(Chunk& c, std::vector<BatchEvent>& events) {
   totals_.closest = counters_host_->closest;
   totals_.any = counters_host_->any;
   totals_.status |= counters_host_->status;
-  for (const SegmentPlan& s : c.segs) {
+  for (size_t j = 0; j < c.segs.size(); j++) {
+    const SegmentPlan& s = c.segs[j];
     Request& r = *s.r;
     r.inflight--;
+    const bool copied = s.preview ? r.host_preview != nullptr
+                                  : (c.passes_done[j] > 0 && (c.passes_done[j] == r.d.samples ? r.host_image != nullptr
+                                                                                               : r.host_progress != nullptr));
+    if (copied) r.copying--;
     if (r.cancelled) continue;
     if (s.preview) {
       events.push_back(BatchEvent{r.id, kEventPreview, 0});
-    } else if (s.pass0 + s.passes == r.d.samples && s.pix0 + s.npix == r.pixels()) {
+    } else if (c.passes_done[j] == r.d.samples) {
       r.finished = true;
       events.push_back(BatchEvent{r.id, kEventDone, r.d.samples});
+    } else if (c.passes_done[j] > 0) {
+      events.push_back(BatchEvent{r.id, kEventProgress, c.passes_done[j]});
     }
   }
+  if (inflight_.size() <= 1) copy_pending_ = false;  // this chunk's copies were the last enqueued
   for (auto it = requests_.begin(); it != requests_.end();) {
     Request& r = **it;
     if ((r.finished || r.cancelled) && r.inflight == 0) {

@@ -51,7 +51,7 @@ struct BatchRequestDesc {
   int srgb = 1;
 };
 
-enum BatchEventKind { kEventPreview = 1, kEventDone = 2, kEventFailed = 3 };
+enum BatchEventKind { kEventPreview = 1, kEventDone = 2, kEventProgress = 3 };
 
 struct BatchEvent {
   long long id;
@@ -81,7 +81,10 @@ class BatchEngine {
   cudaError_t set_scene(int slot, const DScene& scene, int lights);
   bool scene_busy(int slot) const;
   // Queues a request; its buffers are taken from the arena when it is admitted.
-  long long submit(const BatchRequestDesc& d, uint8_t* host_image, uint8_t* host_preview);
+  // `host_progress` (or nullptr) receives the image after every chunk that
+  // completes a pass short of the last.
+  long long submit(const BatchRequestDesc& d, uint8_t* host_image, uint8_t* host_preview,
+                   uint8_t* host_progress = nullptr);
   // Stops a request; its buffers return to the arena once no chunk uses them.
   bool cancel(long long id);
   // Launches the next chunk (if any request has work), then waits for the
@@ -96,6 +99,10 @@ class BatchEngine {
   // Limits a chunk to `paths` paths (<= capacity): smaller chunks bound the
   // latency of a new request's preview under load.
   void set_chunk_paths(int paths) { chunk_paths_ = paths; }
+  // Traversal kernel variant (traversal_variant_info); waits for chunks in
+  // flight and rebuilds the graph on the next launch.
+  cudaError_t set_variant(int variant);
+  int variant() const { return grids_.variant; }
 
  private:
   struct Request {
@@ -103,6 +110,7 @@ class BatchEngine {
     BatchRequestDesc d;
     uint8_t* host_image = nullptr;    // final image
     uint8_t* host_preview = nullptr;  // block preview
+    uint8_t* host_progress = nullptr; // intermediate images
     float4* sum = nullptr;
     uint8_t* image = nullptr;
     bool admitted = false, cancelled = false, finished = false;
@@ -110,6 +118,7 @@ class BatchEngine {
     int next_pass = 0;        // first pass not yet scheduled
     int next_pix = 0;         // first pixel of next_pass not yet scheduled (split passes)
     int inflight = 0;         // chunks in flight that hold a segment of this request
+    int copying = 0;          // chunks in flight copying this request's image to the host
     long long pixels() const { return static_cast<long long>(d.fp.width) * d.fp.height; }
   };
   struct SegmentPlan {
@@ -122,6 +131,9 @@ class BatchEngine {
     std::vector<SegmentPlan> segs;
     cudaEvent_t start = nullptr, done = nullptr, copied = nullptr;
     bool copies = false;
+    // Per segment: the pass count its image holds when the chunk ends, if
+    // the chunk completes a pass of the request (else 0).
+    std::vector<int> passes_done;
   };
 
   cudaError_t ensure_graph();
@@ -154,6 +166,10 @@ class BatchEngine {
   long long next_id_ = 1;
   std::deque<std::unique_ptr<Request>> requests_;  // submission order
   std::deque<Chunk> inflight_;
+  // Copy-stream event of the last chunk that copied images to the host: the
+  // next chunk waits for it, so no kernel rewrites an image being copied.
+  cudaEvent_t last_copy_ = nullptr;
+  bool copy_pending_ = false;
   int next_slot_ = 0;
   BatchTotals totals_;
 };

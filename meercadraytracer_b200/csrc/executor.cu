@@ -203,6 +203,7 @@ struct mcrt_executor {
   std::unordered_map<int, std::unique_ptr<TextureGpu>> textures;
   PathBuffers paths;
   int capacity = 1 << 24;  // paths in flight: 16M, about 9 GB of path state with 5 lights
+  int variant = 0;         // traversal kernels' (block, short stack) variant
   bool timed = false;
   RenderStats stats;
   double ms_total = 0;
@@ -340,6 +341,7 @@ void run_frame(mcrt_executor* ex, FrameParams fp, int total, int passes, ChunkCt
     fp.npix = std::min(cap, total - p0);
     ctx.fp = fp;
     Wavefront wf;
+    wf.variant = ex->variant;
     cuda_check(wf.run(scene, fp, passes, ex->paths, ex->stream, &ex->stats, ex->timed, chunk, &ctx), "render");
   }
   cuda_check(cudaEventRecord(ex->ev1, ex->stream), "cudaEventRecord");
@@ -1000,6 +1002,24 @@ int32_t mcrt_set_capacity(mcrt_executor* ex, int32_t paths) {
   });
 }
 
+int32_t mcrt_traversal_variants(int32_t max, int32_t* blocks, int32_t* stacks, int32_t* count) {
+  return guard([&] {
+    if (max < 0 || (max > 0 && (!blocks || !stacks))) fail(MCRT_ERR_INVALID, "bad output arrays");
+    const int n = traversal_variant_count();
+    for (int i = 0; i < n && i < max; i++) traversal_variant_info(i, &blocks[i], &stacks[i]);
+    if (count) *count = n;
+  });
+}
+
+int32_t mcrt_set_traversal(mcrt_executor* ex, int32_t block, int32_t stack) {
+  return guard([&] {
+    checked(ex);
+    const int v = find_traversal_variant(block, stack);
+    if (v < 0) fail(MCRT_ERR_INVALID, "no traversal kernels compiled for this block size and stack depth");
+    ex->variant = v;
+  });
+}
+
 int32_t mcrt_get_stats(mcrt_executor* ex, mcrt_stats* out) {
   return guard([&] {
     checked(ex);
@@ -1107,7 +1127,7 @@ int64_t submit_request(mcrt_batch* b, const mcrt_request* r) {
   if (pix * 20 + 512 > b->engine.arena().capacity())
     fail(MCRT_ERR_LIMIT, "the request's buffers exceed the batch's memory budget");
   d.scene = scene_slot(b, r);
-  const long long id = b->engine.submit(d, r->image, r->preview_image);
+  const long long id = b->engine.submit(d, r->image, r->preview_image, r->progress_image);
   if (id < 0) fail(MCRT_ERR_INVALID, "request rejected");
   return id;
 }
@@ -1145,6 +1165,15 @@ int32_t mcrt_batch_set_chunk(mcrt_batch* b, int32_t paths) {
     checked_batch(b);
     if (paths < 0) fail(MCRT_ERR_INVALID, "negative chunk size");
     b->engine.set_chunk_paths(paths);
+  });
+}
+
+int32_t mcrt_batch_set_traversal(mcrt_batch* b, int32_t block, int32_t stack) {
+  return guard([&] {
+    checked_batch(b);
+    const int v = find_traversal_variant(block, stack);
+    if (v < 0) fail(MCRT_ERR_INVALID, "no traversal kernels compiled for this block size and stack depth");
+    cuda_check(b->engine.set_variant(v), "batch traversal variant");
   });
 }
 

@@ -21,6 +21,9 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "render.cuh"
 #include "traverse.cuh"
@@ -142,12 +145,14 @@ struct ExtendQuery {
   }
 };
 
-__global__ void __launch_bounds__(kBlock) k_extend(DScene sc, PathState ps, const int* __restrict__ queue, int n,
-                                                   Counters* cnt) {
-  __shared__ int stack_mem[kShort * kBlock];
-  TravStack st;
+// B threads per block, S short-stack entries per thread (a traversal variant).
+template <int B, int S>
+__global__ void __launch_bounds__(B) k_extend(DScene sc, PathState ps, const int* __restrict__ queue, int n,
+                                              Counters* cnt) {
+  __shared__ int stack_mem[S * B];
+  TravStackT<S> st;
   st.smem = stack_mem + threadIdx.x;
-  st.stride = kBlock;
+  st.stride = B;
   st.sp = 0;
   unsigned status = 0;
   ExtendQuery q{sc, ps, queue, 0, {}};
@@ -767,11 +772,12 @@ struct ShadowQuery {
   }
 };
 
-__global__ void __launch_bounds__(kBlock) k_shadow(DScene sc, PathState ps, int n, int capacity, Counters* cnt) {
-  __shared__ int stack_mem[kShort * kBlock];
-  TravStack st;
+template <int B, int S>
+__global__ void __launch_bounds__(B) k_shadow(DScene sc, PathState ps, int n, int capacity, Counters* cnt) {
+  __shared__ int stack_mem[S * B];
+  TravStackT<S> st;
   st.smem = stack_mem + threadIdx.x;
-  st.stride = kBlock;
+  st.stride = B;
   st.sp = 0;
   unsigned status = 0;
   ShadowQuery q{sc, ps, capacity, &status};
@@ -1060,23 +1066,67 @@ struct Timer {
 
 inline int blocks_for(long long n, int block) { return static_cast<int>((n + block - 1) / block); }
 
-// Blocks of a persistent traversal launch: enough to fill every SM at the
-// kernel's occupancy, fewer when there is less work.
-template <class K>
-int persistent_blocks(K kernel, long long n) {
-  static int per_device[64][2] = {};  // cached (SMs, blocks per SM) per device
+// Blocks of a persistent launch of `kernel` with `block` threads: enough to
+// fill every SM at the kernel's occupancy (cached per device and kernel),
+// fewer when there is less work.
+int resident_limit(const void* kernel, int block) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> cache;
   int dev = 0;
   cudaGetDevice(&dev);
-  int* c = per_device[dev & 63];
-  if (c[0] == 0) {
-    cudaDeviceGetAttribute(&c[0], cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c[1], kernel, kBlock, 0);
-    if (c[1] < 1) c[1] = 1;
-  }
-  return static_cast<int>(std::min<long long>(blocks_for(n, kBlock), static_cast<long long>(c[0]) * c[1]));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find({kernel, dev});
+  if (it != cache.end()) return it->second;
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+  const int r = std::max(1, sms) * std::max(1, per_sm);
+  cache[{kernel, dev}] = r;
+  return r;
 }
 
+template <class K>
+int persistent_blocks(K kernel, long long n, int block = kBlock) {
+  const int limit = resident_limit(reinterpret_cast<const void*>(kernel), block);
+  return static_cast<int>(std::min<long long>(blocks_for(n, block), limit));
+}
+
+// The traversal kernels compiled for each variant (block size, short-stack
+// depth); the autotuner picks one per scene and workload.
+using ExtendFn = void (*)(DScene, PathState, const int*, int, Counters*);
+using ShadowFn = void (*)(DScene, PathState, int, int, Counters*);
+
+struct PlainVariant {
+  int block, stack;
+  ExtendFn extend;
+  ShadowFn shadow;
+};
+
+#define MCRT_PLAIN_VARIANT(B, S) PlainVariant{B, S, k_extend<B, S>, k_shadow<B, S>}
+const PlainVariant kPlainVariants[] = {
+    MCRT_PLAIN_VARIANT(128, 16), MCRT_PLAIN_VARIANT(64, 16), MCRT_PLAIN_VARIANT(128, 8),
+    MCRT_PLAIN_VARIANT(128, 24), MCRT_PLAIN_VARIANT(256, 8), MCRT_PLAIN_VARIANT(256, 16),
+};
+#undef MCRT_PLAIN_VARIANT
+constexpr int kVariantCount = static_cast<int>(sizeof(kPlainVariants) / sizeof(kPlainVariants[0]));
+
+const PlainVariant& plain_variant(int v) { return kPlainVariants[(v >= 0 && v < kVariantCount) ? v : 0]; }
+
 }  // namespace
+
+int traversal_variant_count() { return kVariantCount; }
+
+void traversal_variant_info(int v, int* block, int* stack) {
+  const PlainVariant& p = plain_variant(v);
+  if (block) *block = p.block;
+  if (stack) *stack = p.stack;
+}
+
+int find_traversal_variant(int block, int stack) {
+  for (int i = 0; i < kVariantCount; i++)
+    if (kPlainVariants[i].block == block && kPlainVariants[i].stack == stack) return i;
+  return -1;
+}
 
 cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, PathBuffers& buffers,
                            cudaStream_t stream, RenderStats* stats, bool timed,
@@ -1092,6 +1142,7 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
   fp.capacity = cap;
   fp.slot_count = buffers.slots();
   Timer tm(timed, stream);
+  const PlainVariant& tv = plain_variant(variant);
   RenderStats local;
   RenderStats& st = stats ? *stats : local;
   cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(Counters), stream);
@@ -1116,7 +1167,7 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
       }
       cudaMemsetAsync(&cnt->fetch, 0, sizeof(unsigned int), stream);
       tm.start();
-      k_extend<<<persistent_blocks(k_extend, n), kBlock, 0, stream>>>(scene, ps, ps.queue[cur], n, cnt);
+      tv.extend<<<persistent_blocks(tv.extend, n, tv.block), tv.block, 0, stream>>>(scene, ps, ps.queue[cur], n, cnt);
       tm.stop(st.ms_extend, st.n_extend);
       st.closest_rays += n;
       cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), stream);
@@ -1132,7 +1183,8 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
       if (n_shadow > 0) {
         cudaMemsetAsync(&cnt->fetch, 0, sizeof(unsigned int), stream);
         tm.start();
-        k_shadow<<<persistent_blocks(k_shadow, n_shadow), kBlock, 0, stream>>>(scene, ps, n_shadow, cap, cnt);
+        tv.shadow<<<persistent_blocks(tv.shadow, n_shadow, tv.block), tv.block, 0, stream>>>(scene, ps, n_shadow, cap,
+                                                                                             cnt);
         tm.stop(st.ms_shadow, st.n_shadow);
         st.any_rays += n_shadow;
         st.launches++;
@@ -1169,7 +1221,9 @@ cudaError_t primary_hits(const DScene& scene, FrameParams fp, PathBuffers& buffe
   fp.slot_count = buffers.slots();
   k_raygen<<<blocks_for(n, kBlock), kBlock, 0, stream>>>(fp, ps, n);
   cudaMemsetAsync(&buffers.counters()->fetch, 0, sizeof(unsigned int), stream);
-  k_extend<<<persistent_blocks(k_extend, n), kBlock, 0, stream>>>(scene, ps, ps.queue[0], n, buffers.counters());
+  const PlainVariant& tv = plain_variant(0);
+  tv.extend<<<persistent_blocks(tv.extend, n, tv.block), tv.block, 0, stream>>>(scene, ps, ps.queue[0], n,
+                                                                                  buffers.counters());
   return cudaGetLastError();
 }
 
@@ -1232,15 +1286,16 @@ __global__ void __launch_bounds__(kBlock) k_batch_raygen(const BatchTables* __re
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_batch_extend(DScene sc, int s, BatchTables* t, PathState ps,
-                                                         BatchCounters* bc) {
+template <int B, int S>
+__global__ void __launch_bounds__(B) k_batch_extend(DScene sc, int s, BatchTables* t, PathState ps,
+                                                    BatchCounters* bc) {
   SceneQueues* sq = &t->scenes[s];
   const int n = static_cast<int>(sq->count);
   if (n == 0) return;
-  __shared__ int stack_mem[kShort * kBlock];
-  TravStack st;
+  __shared__ int stack_mem[S * B];
+  TravStackT<S> st;
   st.smem = stack_mem + threadIdx.x;
-  st.stride = kBlock;
+  st.stride = B;
   st.sp = 0;
   unsigned status = 0;
   ExtendQuery q{sc, ps, ps.queue[t->iteration & 1] + sq->base, 0, {}};
@@ -1261,15 +1316,16 @@ __global__ void __launch_bounds__(kBlock) k_batch_shade(DScene sc, int s, BatchT
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_batch_shadow(DScene sc, int s, BatchTables* t, PathState ps, int capacity,
-                                                         int slots, BatchCounters* bc) {
+template <int B, int S>
+__global__ void __launch_bounds__(B) k_batch_shadow(DScene sc, int s, BatchTables* t, PathState ps, int capacity,
+                                                    int slots, BatchCounters* bc) {
   SceneQueues* sq = &t->scenes[s];
   const int n = static_cast<int>(sq->shadow_count);
   if (n == 0) return;
-  __shared__ int stack_mem[kShort * kBlock];
-  TravStack st;
+  __shared__ int stack_mem[S * B];
+  TravStackT<S> st;
   st.smem = stack_mem + threadIdx.x;
-  st.stride = kBlock;
+  st.stride = B;
   st.sp = 0;
   unsigned status = 0;
   PathState pq = ps;
@@ -1365,21 +1421,38 @@ __global__ void __launch_bounds__(256) k_batch_accumulate(const BatchTables* __r
   }
 }
 
-int resident_blocks(const void* kernel, int block) {
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
-  return std::max(1, sms * std::max(1, per_sm));
-}
+int resident_blocks(const void* kernel, int block) { return resident_limit(kernel, block); }
+
+using BatchExtendFn = void (*)(DScene, int, BatchTables*, PathState, BatchCounters*);
+using BatchShadowFn = void (*)(DScene, int, BatchTables*, PathState, int, int, BatchCounters*);
+
+struct BatchVariant {
+  int block, stack;
+  BatchExtendFn extend;
+  BatchShadowFn shadow;
+};
+
+// The same variants, in the same order, as kPlainVariants.
+#define MCRT_BATCH_VARIANT(B, S) BatchVariant{B, S, k_batch_extend<B, S>, k_batch_shadow<B, S>}
+const BatchVariant kBatchVariants[] = {
+    MCRT_BATCH_VARIANT(128, 16), MCRT_BATCH_VARIANT(64, 16), MCRT_BATCH_VARIANT(128, 8),
+    MCRT_BATCH_VARIANT(128, 24), MCRT_BATCH_VARIANT(256, 8), MCRT_BATCH_VARIANT(256, 16),
+};
+#undef MCRT_BATCH_VARIANT
+static_assert(sizeof(kBatchVariants) / sizeof(kBatchVariants[0]) == kVariantCount, "variant tables differ");
+
+const BatchVariant& batch_variant(int v) { return kBatchVariants[(v >= 0 && v < kVariantCount) ? v : 0]; }
 
 }  // namespace
 
-cudaError_t batch_grids(BatchGrids* g) {
+cudaError_t batch_grids(BatchGrids* g, int variant) {
+  const BatchVariant& bv = batch_variant(variant);
+  g->variant = (variant >= 0 && variant < kVariantCount) ? variant : 0;
+  g->block = bv.block;
   g->raygen = resident_blocks(reinterpret_cast<const void*>(k_batch_raygen), kBlock);
-  g->extend = resident_blocks(reinterpret_cast<const void*>(k_batch_extend), kBlock);
+  g->extend = resident_blocks(reinterpret_cast<const void*>(bv.extend), bv.block);
   g->shade = resident_blocks(reinterpret_cast<const void*>(k_batch_shade), kBlock);
-  g->shadow = resident_blocks(reinterpret_cast<const void*>(k_batch_shadow), kBlock);
+  g->shadow = resident_blocks(reinterpret_cast<const void*>(bv.shadow), bv.block);
   g->resolve = resident_blocks(reinterpret_cast<const void*>(k_batch_resolve), kBlock);
   g->accumulate = resident_blocks(reinterpret_cast<const void*>(k_batch_accumulate), 256);
   return cudaGetLastError();
@@ -1393,10 +1466,11 @@ cudaError_t launch_batch_raygen(const BatchTables* t, const PathState& ps, const
 cudaError_t launch_batch_iteration(const DScene* scenes, int nscenes, BatchTables* t, const PathState& ps,
                                    int capacity, int slots, BatchCounters* counters, const BatchGrids& g, bool graph,
                                    cudaGraphConditionalHandle handle, cudaStream_t s) {
-  for (int i = 0; i < nscenes; i++) k_batch_extend<<<g.extend, kBlock, 0, s>>>(scenes[i], i, t, ps, counters);
+  const BatchVariant& bv = batch_variant(g.variant);
+  for (int i = 0; i < nscenes; i++) bv.extend<<<g.extend, bv.block, 0, s>>>(scenes[i], i, t, ps, counters);
   for (int i = 0; i < nscenes; i++) k_batch_shade<<<g.shade, kBlock, 0, s>>>(scenes[i], i, t, ps, slots);
   for (int i = 0; i < nscenes; i++)
-    k_batch_shadow<<<g.shadow, kBlock, 0, s>>>(scenes[i], i, t, ps, capacity, slots, counters);
+    bv.shadow<<<g.shadow, bv.block, 0, s>>>(scenes[i], i, t, ps, capacity, slots, counters);
   for (int i = 0; i < nscenes; i++) k_batch_resolve<<<g.resolve, kBlock, 0, s>>>(scenes[i], i, t, ps, capacity);
   k_batch_advance<<<1, 32, 0, s>>>(t, nscenes, counters, graph ? 1 : 0, handle);
   return cudaGetLastError();

@@ -111,6 +111,7 @@ class PathBuffers {
 // can consume the samples. Returns a CUDA error, or cudaSuccess.
 class Wavefront {
  public:
+  int variant = 0;  // traversal variant (see traversal_variant_info)
   cudaError_t run(const DScene& scene, FrameParams fp, int passes, PathBuffers& buffers, cudaStream_t stream,
                   RenderStats* stats, bool timed,
                   cudaError_t (*on_chunk)(void* ctx, int first_pass, int pass_count), void* ctx);
@@ -174,12 +175,20 @@ struct BatchCounters {
   unsigned more;               // set by the iteration step when paths remain (host-driven loop)
 };
 
-// Grid sizes of the batched kernels on the current device.
+// Grid sizes of the batched kernels on the current device, for a traversal variant.
 struct BatchGrids {
   int raygen, extend, shade, shadow, resolve, accumulate;
+  int variant, block;
 };
 
-cudaError_t batch_grids(BatchGrids* g);
+cudaError_t batch_grids(BatchGrids* g, int variant = 0);
+
+// Traversal variants: the closest-hit and shadow kernels compiled for several
+// (threads per block, shared-memory short-stack entries per thread) pairs.
+// Variant 0 is the default (128, 16).
+int traversal_variant_count();
+void traversal_variant_info(int variant, int* block, int* stack);
+int find_traversal_variant(int block, int stack);  // -1 when not compiled
 // Camera rays of every segment of the chunk.
 cudaError_t launch_batch_raygen(const BatchTables* t, const PathState& ps, const BatchGrids& g, cudaStream_t s);
 // One wavefront iteration over every scene: closest hits, shading, shadow

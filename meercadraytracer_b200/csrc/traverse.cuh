@@ -35,7 +35,7 @@
 
 namespace mcrt {
 
-constexpr int kShort = 16;  // shared-memory stack entries per thread
+constexpr int kShort = 16;  // default shared-memory stack entries per thread
 constexpr int kSentinel = 0x7fffffff;  // empty stack / finished ray
 constexpr int kLeafEnd = 1 << 16;      // in tris[3k].w: last triangle of its leaf
 constexpr int kRefill = 8;             // refill a warp's finished lanes once this many are idle
@@ -152,17 +152,19 @@ MCRT_D NodeRefs load_node(const DNode* nodes, int i) {
   return n;
 }
 
-// Two-level traversal stack: kShort entries in shared memory, the rest local.
-struct TravStack {
+// Two-level traversal stack: SHORT entries in shared memory, the rest local.
+template <int SHORT>
+struct TravStackT {
+  static_assert(SHORT > 0 && SHORT < kStackMax, "short stack depth out of range");
   int* smem;  // this thread's column: entry i at smem[i * stride]
   int stride;
   int sp;
-  int spill[kStackMax - kShort];
+  int spill[kStackMax - SHORT];
   MCRT_D bool push(int v) {
-    if (sp < kShort) {
+    if (sp < SHORT) {
       smem[sp * stride] = v;
     } else if (sp < kStackMax) {
-      spill[sp - kShort] = v;
+      spill[sp - SHORT] = v;
     } else {
       return false;
     }
@@ -173,9 +175,10 @@ struct TravStack {
   MCRT_D int pop() {
     if (sp == 0) return kSentinel;
     --sp;
-    return sp < kShort ? smem[sp * stride] : spill[sp - kShort];
+    return sp < SHORT ? smem[sp * stride] : spill[sp - SHORT];
   }
 };
+using TravStack = TravStackT<kShort>;
 
 MCRT_D void load_tri(const DScene& sc, int k, V3& a, V3& b, V3& c, float4& w0, float4& w1) {
   const float4* p = sc.tris + 3 * static_cast<size_t>(k);
@@ -206,8 +209,8 @@ MCRT_D int root_ref(const DScene& sc) { return sc.root_count > 0 ? ~0 : 0; }
 //   bool leaf(int first)      test the leaf starting at triangle `first`;
 //                             false ends the query (any hit: blocked)
 //   void finish()             write the query's result
-template <class Q>
-MCRT_D void traverse_persistent(const DScene& sc, Q& q, int n, unsigned* counter, TravStack& st,
+template <class Q, class ST>
+MCRT_D void traverse_persistent(const DScene& sc, Q& q, int n, unsigned* counter, ST& st,
                                 unsigned& status) {
   const unsigned lane = threadIdx.x & 31;
   const bool empty = sc.tri_count == 0;

@@ -330,6 +330,10 @@ class GpuExecutor:
     def set_capacity(self, paths: int) -> None:
         call("mcrt_set_capacity", self._h, int(paths))
 
+    def set_traversal(self, block: int, stack: int) -> None:
+        """Traversal kernels by threads per block and short-stack depth (_lib.traversal_variants())."""
+        call("mcrt_set_traversal", self._h, int(block), int(stack))
+
     def stats(self) -> Dict[str, Any]:
         s = mcrt_stats()
         call("mcrt_get_stats", self._h, C.byref(s))

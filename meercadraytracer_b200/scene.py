@@ -286,6 +286,7 @@ class BufferGeometry:
     groups: List[Tuple[int, int, int]] = field(default_factory=list)  # (start, count, materialIndex)
     draw_start: int = 0
     draw_count: float = math.inf
+    version: int = 0  # bump after editing the arrays in place (three.js attribute.needsUpdate)
 
     def add_group(self, start: int, count: int, material_index: int) -> None:
         self.groups.append((start, count, material_index))

@@ -13,9 +13,16 @@ here and documented in DESIGN.md.
                  grid, mixed Standard / Physical / Phong materials, half with
                  256 x 256 noise albedo maps; 1920 x 1080, 64 spp, GI on,
                  4 bounces, ACES, sRGB.
+  mid_scene(grid=32)  the serving loop's large version: 1,024 icospheres,
+                 5,242,880 triangles.
+  soup_scene()   2,000,000 random triangles, edge lengths U(0.01, 0.2), in a
+                 20^3 box, Lambert albedo U(0, 1)^3 per triangle (vertex colours).
+  orbit_camera() the serving loop's clients: a camera on a circle around a
+                 scene, aimed at its centre.
 """
 from __future__ import annotations
 
+import functools
 import math
 from dataclasses import dataclass, field
 from typing import Any, Dict, List, Tuple
@@ -79,9 +86,22 @@ def small_scene(seed: int = SEED_BASE + 0) -> BenchScene:
 
 
 # ------------------------------------------------------------- icospheres
+@functools.lru_cache(maxsize=8)
+def _icosphere(subdivisions: int) -> Tuple[np.ndarray, np.ndarray]:
+    v, f = _make_icosphere(subdivisions)
+    v.setflags(write=False)
+    f.setflags(write=False)
+    return v, f
+
+
 def icosphere(subdivisions: int) -> Tuple[np.ndarray, np.ndarray]:
     """Unit icosphere: an icosahedron whose faces are split in four `subdivisions`
     times, new vertices pushed to the sphere. Returns (vertices [v, 3], faces [f, 3])."""
+    v, f = _icosphere(subdivisions)
+    return v.copy(), f.copy()
+
+
+def _make_icosphere(subdivisions: int) -> Tuple[np.ndarray, np.ndarray]:
     t = (1 + math.sqrt(5)) / 2
     verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
              (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
@@ -230,3 +250,53 @@ def mid_scene(seed: int = SEED_BASE + 1, grid: int = 16, subdivisions: int = 4, 
 
 def f_count(subdivisions: int) -> int:
     return 20 * 4 ** subdivisions
+
+
+def soup_scene(seed: int = SEED_BASE + 3, count: int = 2_000_000, box: float = 20.0, width: int = 1280,
+               height: int = 720, samples: int = 64) -> BenchScene:
+    """A random triangle soup: `count` triangles with a random first vertex in the box and
+    edges of length U(0.01, 0.2) in random directions, one Lambert material with a
+    U(0, 1)^3 albedo per triangle as vertex colours; a sun with shadows and a hemisphere light."""
+    rng = np.random.default_rng(seed)
+    v0 = rng.uniform(-box / 2, box / 2, (count, 3))
+
+    def edge() -> np.ndarray:
+        d = rng.normal(size=(count, 3))
+        d /= np.maximum(np.linalg.norm(d, axis=1, keepdims=True), 1e-12)
+        return d * rng.uniform(0.01, 0.2, (count, 1))
+
+    v1, v2 = v0 + edge(), v0 + edge()
+    p = np.stack([v0, v1, v2], axis=1).astype(np.float32)  # [n, 3, 3]
+    fn = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]).astype(np.float64)
+    fn /= np.maximum(np.linalg.norm(fn, axis=1, keepdims=True), 1e-30)
+    n = np.repeat(fn[:, None, :], 3, axis=1).astype(np.float32)
+    albedo = rng.uniform(0, 1, (count, 3))
+    colors = np.repeat(albedo[:, None, :], 3, axis=1).astype(np.float32)
+    geometry = S.BufferGeometry(p.reshape(-1, 3), n.reshape(-1, 3), None, color=colors.reshape(-1, 3))
+    material = S.MeshLambertMaterial(vertex_colors=True, side=S.DoubleSide)
+    scene = S.Scene()
+    scene.add(S.Mesh(geometry, material))
+    sun = S.DirectionalLight(0xffffff, 3)
+    sun.position.set(10, 20, 5)
+    sun.cast_shadow = True
+    scene.add(sun, S.HemisphereLight(0xddeeff, 0x202020, 0.5))
+    camera = S.PerspectiveCamera(50, width / height, 0.1, 2000)
+    camera.position.set(0, 12, 34)
+    camera.look_at(0, 0, 0)
+    camera.update_matrix_world()
+    return BenchScene(f"soup: {count:,} random triangles in a {box:g}^3 box, {width}x{height}, {samples} spp, GI on",
+                      scene, camera, width, height,
+                      {"samples": samples, "global_illumination": True, "max_bounces": 4,
+                       "tone_mapping": S.ACESFilmicToneMapping, "output_color_space": "srgb"}, count)
+
+
+def orbit_camera(radius: float, height: float, angle_deg: float, target: Tuple[float, float, float] = (0, 0, 0),
+                 aspect: float = 16 / 9, fov: float = 50) -> S.PerspectiveCamera:
+    """A perspective camera on a circle of `radius` at `height` above the target, at
+    `angle_deg` around the y axis, looking at the target."""
+    a = math.radians(angle_deg)
+    camera = S.PerspectiveCamera(fov, aspect, 0.1, 4000)
+    camera.position.set(target[0] + radius * math.sin(a), target[1] + height, target[2] + radius * math.cos(a))
+    camera.look_at(*target)
+    camera.update_matrix_world()
+    return camera

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from meercadraytracer_b200 import scenes
-from meercadraytracer_b200.batch import EVENT_DONE, EVENT_PREVIEW, BatchRenderer, RenderRequest
+from meercadraytracer_b200.batch import EVENT_DONE, EVENT_PREVIEW, EVENT_PROGRESS, BatchRenderer, RenderRequest
 from meercadraytracer_b200.compile import compile_camera, compile_scene
 from meercadraytracer_b200.raytrace import as_options, trace_settings
 from meercadraytracer_b200.types import Tile
@@ -148,5 +148,33 @@ def test_cancelled_requests_return_their_memory(two_scenes):
         assert done == [ids[0]]
         assert np.array_equal(renderer.result(ids[0]), _plain(renderer, reqs[0]))
         assert renderer.stats()["arena_used"] == 0
+    finally:
+        renderer.dispose()
+
+
+def test_progress_events_report_completed_passes(two_scenes):
+    # 64 x 48 = 3072 pixels; a 6144-path chunk holds two passes, so a 6-sample render
+    # reports progress at 2 and 4 passes, then done at 6.
+    s_scene, s_cam, s_st = two_scenes[0]
+    w, h = 64, 48
+    renderer = BatchRenderer(capacity=2 * w * h, memory_budget=64 << 20)
+    try:
+        rid = renderer.submit(RenderRequest(s_scene, s_cam, w, h, s_st, 6, progress=True))
+        seen, frames = [], []
+        for _ in range(1000):
+            events, idle = renderer.step()
+            for e in events:
+                seen.append((e[1], e[2]))
+                if e[1] == EVENT_PROGRESS:
+                    frames.append((e[2], renderer.progress(rid).copy()))
+            if idle:
+                break
+        assert seen == [(EVENT_PROGRESS, 2), (EVENT_PROGRESS, 4), (EVENT_DONE, 6)]
+        plain = {n: _plain(renderer, RenderRequest(s_scene, s_cam, w, h, s_st, n)) for n in (2, 4, 6)}
+        # The progress image holds at least the passes the event reports (a later chunk's
+        # copy may have refreshed it before the host looked).
+        for n, img in frames:
+            assert any(np.array_equal(img, plain[k]) for k in plain if k >= n)
+        assert np.array_equal(renderer.result(rid), plain[6])
     finally:
         renderer.dispose()
