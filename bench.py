@@ -243,6 +243,16 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     def frame() -> None:
         ex.raytrace_device(compiled, cam, w, h, st, spp, srgb, image.data_ptr())
 
+    tuned: Dict[str, Any] = {}
+    if not args.no_tune:
+        # The autotuner picks the traversal variant and the path pool on the same scene and
+        # image at an eighth of the samples (outside the timed region).
+        from meercadraytracer_b200 import autotune
+
+        choice = autotune.tune_plain(ex, compiled, cam, st, w, h, max(2, spp // 8),
+                                     capacities=(1 << 22, 1 << 23, 1 << 24) if not args.capacity else (args.capacity,))
+        tuned = {"block": choice.block, "stack": choice.stack, "capacity": choice.capacity,
+                 "timings_ms": choice.timings}
     for _ in range(args.warmup):
         frame()
     # Timed region: K frames, device time from the library's CUDA events.
@@ -322,6 +332,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         "config": {"workload": bench.name, "triangles": bench.triangles, "width": w, "height": h, "spp": spp,
                    "rays_per_step": rays / args.steps, "l2": "flushed between steps (512 MiB write)",
                    "parallelism": "replicas" if world > 1 else "single GPU", "path_state_bytes": ex.stats()["path_bytes"],
+                   "autotuned": tuned,
                    "compile_s": {"flatten_host": round(t_flat, 3), "gpu_bvh_compile": round(t_build, 3),
                                  "upload": round(t_upload, 3)}},
         "wall_s_timed": round(wall, 3),
@@ -352,6 +363,8 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                                 "sample": f"{base['pixels']} random pixels x {spp} passes ({base['rays']} rays, "
                                           f"{base['seconds']:.1f} s) of the same workload on the oracle, a C++ "
                                           f"restatement of the reference's TypeScript path (no Node.js here)"}
+    if world == 1 and not args.no_large:
+        line["large"] = run_large(local, args.large_count, args.large_frames)
     if world == 1 and not (args.no_batch and args.no_serve):
         # The batched and served forms of the same path, beside the plain number.
         from meercadraytracer_b200 import scenes as SC
@@ -417,12 +430,17 @@ def run_batched(compiled: Dict[str, Any], device: int, capacity: int, seed: int 
         reqs.append(RenderRequest(compiled[scene], compile_camera(cam), w, h, settings, spp))
     renderer = BatchRenderer(device, capacity, memory_budget=4 << 30)
     try:
+        # The autotuner picks the batch's traversal variant and chunk size on 8 of the requests.
+        from meercadraytracer_b200 import autotune
+
+        choice = autotune.tune_batch(renderer, reqs[:8])
         # Plain: one raytraceCompiled per request, on executors that already hold the scenes.
         plain_imgs = []
         execs = {id(c): renderer.executor(c) for c in compiled.values()}
         for ex in execs.values():
             ex.reset_stats()
             ex.set_capacity(capacity)
+            ex.set_traversal(choice.block, choice.stack)
         for r in reqs[:2]:  # warm-up
             execs[id(r.scene)].raytrace(r.scene, r.camera, r.width, r.height, r.settings, 1, True)
         for ex in execs.values():
@@ -459,6 +477,8 @@ def run_batched(compiled: Dict[str, Any], device: int, capacity: int, seed: int 
             "plain_wall_s": round(plain_wall, 3), "batched_wall_s": round(batch_wall, 3),
             "chunks": int(st1["chunks"] - st0["chunks"]), "graph_launches": int(st1["graph_launches"] - st0["graph_launches"]),
             "capacity": capacity, "images_equal_to_plain": f"{same}/{len(reqs)}",
+            "autotuned": {"block": choice.block, "stack": choice.stack, "chunk": choice.chunk,
+                          "timings_ms": choice.timings},
         }
     finally:
         renderer.dispose()
@@ -482,6 +502,18 @@ def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: 
     try:
         for n in names:
             server.add_scene(n, compiled[n])
+        # The autotuner sizes chunks so one takes about 12 ms on the slowest scene (a new
+        # request's preview waits for at most the chunks in flight), unless given.
+        from meercadraytracer_b200 import autotune
+        from meercadraytracer_b200.batch import RenderRequest
+        from meercadraytracer_b200.compile import compile_camera
+        from meercadraytracer_b200.scenes import orbit_camera
+
+        if not chunk:
+            probes = [RenderRequest(compiled[c.scene], compile_camera(orbit_camera(c.radius, c.height, c.phase,
+                                                                                   aspect=16 / 9)),
+                                    1280, 720, settings, 1) for c in clients[: len(names)]]
+            chunk = autotune.tune_serving_chunk(server.batch, probes, target_ms=12.0).chunk
         # Warm-up: one short request per scene (graph instantiation, first-touch).
         simulate_clients(server, clients[: len(names)], {n: settings for n in names}, duration=0.2, width=320,
                          height=180, samples=2, seed=1)
@@ -491,6 +523,58 @@ def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: 
         return out
     finally:
         server.close()
+
+
+# ------------------------------------------------------ per-frame rebuild
+def run_large(device: int, count: int, frames: int, bins: int = 32) -> Dict[str, Any]:
+    """The large workload: `count` icospheres (20,480 triangles each) under rigid transforms
+    re-drawn every frame; each frame compiles the instances on the GPU (flatten, binned-SAH
+    BVH with `bins` bins, reorder, tangents) and renders 2048 x 2048 at 16 spp, GI on,
+    8 bounces. Two untimed warm-up frames first (allocations)."""
+    import torch
+
+    from meercadraytracer_b200 import scenes as SC
+    from meercadraytracer_b200.compile import compile_camera
+    from meercadraytracer_b200.executors import GpuExecutor
+    from meercadraytracer_b200.raytrace import as_options, output_srgb, sample_count, trace_settings
+
+    L = SC.large_scene(count=count)
+    o = as_options(L.options)
+    st, spp, srgb = trace_settings(o), sample_count(o), output_srgb(o)
+    ex = GpuExecutor(device)
+    try:
+        free0, total_mem = torch.cuda.mem_get_info(device)
+        ex.upload_meshes([L.mesh])
+        sv = ex.send_shading_only(L.shading)
+        cam = compile_camera(L.camera)
+        image = torch.empty(L.width * L.height * 4, dtype=torch.uint8, device=f"cuda:{device}")
+        rows = []
+        warm = 2
+        for k in range(frames + warm):
+            t0 = time.perf_counter()
+            instances = L.frame(k)
+            t_host = time.perf_counter() - t0
+            info, _ = ex.compile_instances(instances, bins=bins)
+            ex.reset_stats()
+            ex.raytrace_resident((info["version"], sv), cam, L.width, L.height, st, spp, srgb,
+                                 device_ptr=image.data_ptr())
+            s = ex.stats()
+            free1, _ = torch.cuda.mem_get_info(device)
+            if k < warm:
+                continue  # warm-up: first allocations of the builder, geometry and path buffers
+            rays = s["closest_rays"] + s["any_rays"]
+            rows.append({"frame": k, "instances_host_ms": round(1e3 * t_host, 2),
+                         "build_ms": {"flatten": round(info["flatten_ms"], 2), "bvh": round(info["build_ms"], 2),
+                                      "reorder_tangents": round(info["finish_ms"], 2),
+                                      "total_with_pack": round(info["total_ms"], 2)},
+                         "trace_ms": round(s["ms_total"], 2), "mrays_s": round(rays / (s["ms_total"] / 1e3) / 1e6, 1),
+                         "rays": int(rays), "levels": info["levels"], "nodes": info["node_count"],
+                         "hbm_bytes": {"geometry": int(info["geometry_bytes"]), "builder": int(info["build_bytes"]),
+                                       "path_state": int(s["path_bytes"]), "device_used_by_process": int(free0 - free1)}})
+        return {"workload": L.name, "triangles": L.triangles, "bins": bins, "leaf_size": 4, "frames": rows,
+                "hbm_total_bytes": int(total_mem)}
+    finally:
+        ex.dispose()
 
 
 def traffic_from_profile(kernel: str) -> Optional[float]:
@@ -520,6 +604,10 @@ def main() -> None:
     ap.add_argument("--height", type=int, default=0, help="override the image height (profiling runs)")
     ap.add_argument("--spp", type=int, default=0, help="override samples per pixel (profiling runs)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-renders comparison")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default variant and pool)")
+    ap.add_argument("--no-large", action="store_true", help="skip the per-frame rebuild workload")
+    ap.add_argument("--large-count", type=int, default=4096, help="icospheres of the per-frame rebuild workload")
+    ap.add_argument("--large-frames", type=int, default=2, help="timed frames of the per-frame rebuild workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop run")
     ap.add_argument("--batch-capacity", type=int, default=1 << 24, help="path pool of the batch engine")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the served client simulation")

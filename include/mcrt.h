@@ -164,6 +164,73 @@ int32_t mcrt_compile_geometry(mcrt_executor* executor, int32_t count, const doub
                               float* bounds_out, int32_t* nodes_out, uint32_t* order_out, int32_t* node_count_out,
                               double* epsilon_out, int32_t* any_colors);
 
+/* ------------------------------------------------------------------------
+ * Instanced geometry compiled on the device. The reference flattens meshes
+ * on the host (addMesh, src/compile.ts:212-306) and ships the result; here
+ * the meshes are uploaded once and every rebuild (a frame whose instances
+ * moved) runs the flatten, the BVH build, the reorder, tangents and epsilon
+ * on the GPU, leaving the geometry resident with no host round trip.
+ * ------------------------------------------------------------------------ */
+typedef struct mcrt_mesh {
+  int32_t vertex_count;
+  int32_t index_count;      /* 0: not indexed (vertex_count a multiple of 3) */
+  const float* position;    /* 3 floats per vertex */
+  const float* normal;      /* 3 floats per vertex, or NULL: face normals */
+  const float* uv;          /* 2 floats per vertex, or NULL: zeros */
+  const uint32_t* index;    /* index_count entries, or NULL */
+} mcrt_mesh;
+
+typedef struct mcrt_instance {
+  double world[16];         /* column-major world matrix (matrixWorld, times instanceMatrix) */
+  int32_t mesh;             /* index into the uploaded meshes */
+  uint32_t material;        /* material index of all its triangles */
+  uint8_t flags;            /* TRI_OPAQUE | TRI_CAST_SHADOW | TRI_RECEIVE_SHADOW */
+  uint8_t side;             /* FrontSide 0, BackSide 1, DoubleSide 2 */
+  uint8_t flat_shading;     /* 1: face normals */
+  uint8_t pad_[5];
+} mcrt_instance;
+
+typedef struct mcrt_build_info {
+  double flatten_ms, build_ms, finish_ms, total_ms;  /* device times: flatten, BVH, reorder + tangents, all */
+  int32_t triangle_count, node_count, levels, bins;
+  uint64_t geometry_bytes;  /* HBM of the resident geometry */
+  uint64_t build_bytes;     /* HBM the builder keeps between builds */
+} mcrt_build_info;
+
+/* Host arrays sized for the triangle count n (and 2n - 1 nodes) that
+ * receive the compiled geometry in the CompiledGeometry layout; any pointer
+ * may be NULL. The counts and epsilon are written back. */
+typedef struct mcrt_compiled_out {
+  float* triangles;
+  float* normals;
+  float* uvs;
+  float* tangents;
+  uint32_t* materials;
+  uint8_t* flags;
+  uint8_t* sides;
+  float* bounds;
+  int32_t* nodes;
+  uint32_t* order;
+  double epsilon;
+  int32_t triangle_count;
+  int32_t node_count;
+} mcrt_compiled_out;
+
+/* Uploads the meshes that instances refer to, replacing earlier ones. No
+ * counterpart in the reference (it reads three.js buffers directly). */
+int32_t mcrt_upload_meshes(mcrt_executor* executor, int32_t count, const mcrt_mesh* meshes);
+
+/* compileGeometry (src/compile.ts:327-432) of `count` instances on the GPU,
+ * meshes in instance order and triangles in index order as addMesh emits
+ * them, with a binned-SAH BVH of `bins` bins per axis (buildBvh's 16 keeps
+ * the reference's tree; up to 32). The result becomes the resident geometry
+ * under `version`, as after mcrt_send_geometry. `info` (or NULL) receives
+ * times and memory; `out` (or NULL) the compiled arrays. Vertex colours and
+ * geometry groups are not part of this path. */
+int32_t mcrt_compile_instances(mcrt_executor* executor, int32_t version, int32_t count,
+                               const mcrt_instance* instances, int32_t bins, mcrt_build_info* info,
+                               mcrt_compiled_out* out);
+
 /* Kernel timing with CUDA events on the executor's stream (adds a sync per
  * kernel; for profiling only). */
 int32_t mcrt_set_timing(mcrt_executor* executor, int32_t enabled);

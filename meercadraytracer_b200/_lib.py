@@ -83,6 +83,9 @@ SIGNATURES = {
     "mcrt_compile_geometry": (_i32, [_vp, _i32, _P(_d), _P(_d), _P(_d), _P(_d), _P(_u8), _P(_u32), _P(_u8), _P(_u8),
                                      _P(_f), _P(_f), _P(_f), _P(_f), _P(_f), _P(_u32), _P(_u8), _P(_u8), _P(_f),
                                      _P(_i32), _P(_u32), _P(_i32), _P(_d), _P(_i32)]),
+    "mcrt_upload_meshes": (_i32, [_vp, _i32, _P(abi.mcrt_mesh)]),
+    "mcrt_compile_instances": (_i32, [_vp, _i32, _i32, _P(abi.mcrt_instance), _i32, _P(abi.mcrt_build_info),
+                                      _P(abi.mcrt_compiled_out)]),
     "mcrt_set_timing": (_i32, [_vp, _i32]),
     "mcrt_set_capacity": (_i32, [_vp, _i32]),
     "mcrt_traversal_variants": (_i32, [_i32, _P(_i32), _P(_i32), _P(_i32)]),

@@ -151,6 +151,38 @@ class mcrt_batch_stats(C.Structure):
     ]
 
 
+class mcrt_mesh(C.Structure):
+    _fields_ = [
+        ("vertex_count", C.c_int32), ("index_count", C.c_int32), ("position", C.POINTER(C.c_float)),
+        ("normal", C.POINTER(C.c_float)), ("uv", C.POINTER(C.c_float)), ("index", C.POINTER(C.c_uint32)),
+    ]
+
+
+class mcrt_instance(C.Structure):
+    _fields_ = [
+        ("world", C.c_double * 16), ("mesh", C.c_int32), ("material", C.c_uint32), ("flags", C.c_uint8),
+        ("side", C.c_uint8), ("flat_shading", C.c_uint8), ("pad_", C.c_uint8 * 5),
+    ]
+
+
+class mcrt_build_info(C.Structure):
+    _fields_ = [
+        ("flatten_ms", C.c_double), ("build_ms", C.c_double), ("finish_ms", C.c_double), ("total_ms", C.c_double),
+        ("triangle_count", C.c_int32), ("node_count", C.c_int32), ("levels", C.c_int32), ("bins", C.c_int32),
+        ("geometry_bytes", C.c_uint64), ("build_bytes", C.c_uint64),
+    ]
+
+
+class mcrt_compiled_out(C.Structure):
+    _fields_ = [
+        ("triangles", C.POINTER(C.c_float)), ("normals", C.POINTER(C.c_float)), ("uvs", C.POINTER(C.c_float)),
+        ("tangents", C.POINTER(C.c_float)), ("materials", C.POINTER(C.c_uint32)), ("flags", C.POINTER(C.c_uint8)),
+        ("sides", C.POINTER(C.c_uint8)), ("bounds", C.POINTER(C.c_float)), ("nodes", C.POINTER(C.c_int32)),
+        ("order", C.POINTER(C.c_uint32)), ("epsilon", C.c_double), ("triangle_count", C.c_int32),
+        ("node_count", C.c_int32),
+    ]
+
+
 def ptr(array: np.ndarray, ctype: Any) -> Any:
     """Pointer to a C-contiguous numpy array's data, or NULL for an empty array."""
     if array is None or array.size == 0:

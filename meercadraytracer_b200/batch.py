@@ -61,6 +61,7 @@ class BatchRenderer:
         self.capacity = int(capacity)
         self._executors: Dict[int, Tuple[CompiledScene, GpuExecutor]] = {}
         self._buffers: Dict[int, Tuple[np.ndarray, Optional[np.ndarray], Optional[np.ndarray]]] = {}
+        self._adopted: set = set()
 
     # ----------------------------------------------------------- scenes
     def executor(self, scene: CompiledScene) -> GpuExecutor:
@@ -72,6 +73,12 @@ class BatchRenderer:
             entry = (scene, ex)
             self._executors[id(scene)] = entry
         return entry[1]
+
+    def adopt(self, scene: CompiledScene, executor: GpuExecutor) -> None:
+        """Uses `executor` (already holding `scene`) for requests on `scene`; the caller keeps
+        ownership (dispose() leaves it alone)."""
+        self._executors[id(scene)] = (scene, executor)
+        self._adopted.add(id(executor))
 
     # ---------------------------------------------------------- requests
     @staticmethod
@@ -177,7 +184,8 @@ class BatchRenderer:
             call("mcrt_batch_destroy", self._h)
             self._h = None
         for _, ex in self._executors.values():
-            ex.dispose()
+            if id(ex) not in self._adopted:
+                ex.dispose()
         self._executors.clear()
 
     def __del__(self):  # pragma: no cover - best effort

@@ -987,6 +987,138 @@ int32_t mcrt_compile_geometry(mcrt_executor* ex, int32_t count, const double* p,
   });
 }
 
+int32_t mcrt_upload_meshes(mcrt_executor* ex, int32_t count, const mcrt_mesh* meshes) {
+  return guard([&] {
+    checked(ex);
+    if (count < 0 || (count > 0 && !meshes)) fail(MCRT_ERR_INVALID, "bad mesh list");
+    std::vector<MeshInput> in(count);
+    for (int i = 0; i < count; i++) {
+      const mcrt_mesh& m = meshes[i];
+      if (m.vertex_count < 0 || (m.vertex_count > 0 && !m.position)) fail(MCRT_ERR_INVALID, "bad mesh positions");
+      if (m.index_count < 0 || m.index_count % 3 != 0 || (m.index_count > 0 && !m.index))
+        fail(MCRT_ERR_INVALID, "bad mesh index");
+      if (m.index_count == 0 && m.vertex_count % 3 != 0) fail(MCRT_ERR_INVALID, "bad mesh vertex count");
+      for (int k = 0; k < m.index_count; k++)
+        if (m.index[k] >= static_cast<uint32_t>(m.vertex_count)) fail(MCRT_ERR_INVALID, "mesh index out of range");
+      in[i] = MeshInput{m.vertex_count, m.position, m.normal, m.uv, m.index_count, m.index};
+    }
+    ex->builder.upload_meshes(count, in.data(), ex->stream);
+  });
+}
+
+int32_t mcrt_compile_instances(mcrt_executor* ex, int32_t version, int32_t count, const mcrt_instance* instances,
+                               int32_t bins, mcrt_build_info* info, mcrt_compiled_out* out) {
+  return guard([&] {
+    checked(ex);
+    if (count < 0 || (count > 0 && !instances)) fail(MCRT_ERR_INVALID, "bad instance list");
+    if (bins < 2 || bins > 32) fail(MCRT_ERR_INVALID, "bins must be 2 to 32");
+    std::vector<InstanceInput> in(count);
+    int64_t max_material = -1;
+    for (int i = 0; i < count; i++) {
+      const mcrt_instance& t = instances[i];
+      InstanceInput d{};
+      std::memcpy(d.world, t.world, sizeof(d.world));
+      d.mesh = t.mesh;
+      d.material = t.material;
+      d.flags = t.flags & 7;
+      d.side = t.side;
+      d.flat_shading = t.flat_shading;
+      in[i] = d;
+      max_material = std::max<int64_t>(max_material, t.material);
+    }
+    const long long total = ex->builder.instance_triangles(count, in.data());
+    if (total < 0) fail(MCRT_ERR_INVALID, "an instance names a mesh that was not uploaded");
+    if (total > (1ll << 30)) fail(MCRT_ERR_LIMIT, "at most 2^30 triangles");
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "event");
+    cuda_check(cudaEventCreate(&e1), "event");
+    cuda_check(cudaEventRecord(e0, ex->stream), "event");
+    ex->have_geometry = false;
+    DeviceGeometry g{};
+    float times[3] = {0, 0, 0};
+    ex->builder.compile_instances(count, in.data(), bins, ex->stream, &g, times);
+    // Make it resident as mcrt_send_geometry does, from device memory.
+    GeometryGpu& G = ex->geo;
+    cudaStream_t s = ex->stream;
+    const int n = g.n, m = g.node_count;
+    G.tri_count = n;
+    G.node_count = m;
+    G.eps = static_cast<float>(g.epsilon);
+    G.root_count = g.root_count;
+    G.max_material = n > 0 ? max_material : -1;
+    G.has_colors = false;
+    if (n > 0) {
+      G.tris.ensure(sizeof(float4) * 3 * n);
+      k_pack_tris<<<blocks(n, 256), 256, 0, s>>>(g.triangles, g.materials, g.flags, g.sides, n, G.tris.as<float4>());
+      G.attrs.ensure(sizeof(float) * 16 * n);
+      k_pack_attrs<<<blocks(n, 256), 256, 0, s>>>(g.normals, g.uvs, n, G.attrs.as<float>());
+      G.tangents.ensure(sizeof(float) * 4 * n);
+      cuda_check(cudaMemcpyAsync(G.tangents.as<float>(), g.tangents, sizeof(float) * 4 * n, cudaMemcpyDeviceToDevice, s),
+                 "copy");
+      k_mark_leaf_ends<<<blocks(m, 256), 256, 0, s>>>(g.nodes, m, G.tris.as<float4>());
+      if (G.root_count == 0) {
+        // A full binary tree of m nodes has (m - 1) / 2 inner nodes.
+        DevBuf flag, index, temp;
+        flag.ensure(sizeof(int) * m);
+        index.ensure(sizeof(int) * m);
+        k_inner_flags<<<blocks(m, 256), 256, 0, s>>>(g.nodes, m, flag.as<int>());
+        size_t temp_bytes = 0;
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, flag.as<int>(), index.as<int>(), m, s), "scan");
+        temp.ensure(temp_bytes);
+        cuda_check(cub::DeviceScan::ExclusiveSum(temp.as<void>(), temp_bytes, flag.as<int>(), index.as<int>(), m, s),
+                   "scan");
+        G.nodes.ensure(sizeof(DNode) * std::max((m - 1) / 2, 1));
+        k_pack_nodes<<<blocks(m, 256), 256, 0, s>>>(g.bounds, g.nodes, index.as<int>(), m, G.nodes.as<DNode>());
+        cuda_check(cudaGetLastError(), "BVH conversion");
+        cuda_check(cudaStreamSynchronize(s), "geometry pack");
+      }
+    }
+    cuda_check(cudaGetLastError(), "geometry pack");
+    if (out) {
+      // The CompiledGeometry arrays, for callers that check or keep them.
+      auto down = [&](void* h, const void* d, size_t bytes) {
+        if (h && bytes) cuda_check(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, s), "download");
+      };
+      const size_t N = static_cast<size_t>(n);
+      down(out->triangles, g.triangles, sizeof(float) * 9 * N);
+      down(out->normals, g.normals, sizeof(float) * 9 * N);
+      down(out->uvs, g.uvs, sizeof(float) * 6 * N);
+      down(out->tangents, g.tangents, sizeof(float) * 4 * N);
+      down(out->materials, g.materials, sizeof(uint32_t) * N);
+      down(out->flags, g.flags, N);
+      down(out->sides, g.sides, N);
+      down(out->bounds, g.bounds, sizeof(float) * 6 * m);
+      down(out->nodes, g.nodes, sizeof(int) * 3 * m);
+      down(out->order, g.order, sizeof(uint32_t) * N);
+      out->epsilon = g.epsilon;
+      out->node_count = m;
+      out->triangle_count = n;
+    }
+    cuda_check(cudaEventRecord(e1, s), "event");
+    cuda_check(cudaEventSynchronize(e1), "compile");
+    float total_ms = 0;
+    cudaEventElapsedTime(&total_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ex->geometry_version = version;
+    ex->have_geometry = true;
+    if (info) {
+      mcrt_build_info r{};
+      r.flatten_ms = times[0];
+      r.build_ms = times[1];
+      r.finish_ms = times[2];
+      r.total_ms = total_ms;
+      r.triangle_count = n;
+      r.node_count = m;
+      r.levels = g.levels;
+      r.bins = bins;
+      r.geometry_bytes = G.bytes();
+      r.build_bytes = ex->builder.device_bytes();
+      *info = r;
+    }
+  });
+}
+
 int32_t mcrt_set_timing(mcrt_executor* ex, int32_t enabled) {
   return guard([&] {
     checked(ex);

@@ -1310,9 +1310,18 @@ __global__ void __launch_bounds__(kBlock) k_batch_shade(DScene sc, int s, BatchT
   const int* qin = ps.queue[cur] + sq->base;
   const StageQueues qs{ps.queue[cur ^ 1] + sq->base, &sq->next_count,
                        ps.shadow_queue + 3ull * sq->base * static_cast<unsigned>(slots), &sq->shadow_count};
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-    const int pid = qin[q];
-    shade_path(sc, t->fp[ps.seg[pid]], ps, pid, qs);
+  // Every lane of a warp runs the same number of iterations and the warp
+  // reconverges after each path: shading diverges by material, and a warp
+  // whose lanes drifted apart across iterations ran each path's code once per
+  // lane group (a third of the lanes active, instruction-cache misses).
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int q = base + threadIdx.x;
+    if (q < n) {
+      const int pid = qin[q];
+      shade_path(sc, t->fp[ps.seg[pid]], ps, pid, qs);
+    }
+    __syncwarp();
   }
 }
 
@@ -1340,9 +1349,14 @@ __global__ void __launch_bounds__(kBlock) k_batch_resolve(DScene sc, int s, Batc
   SceneQueues* sq = &t->scenes[s];
   const int n = static_cast<int>(sq->count);
   const int* qin = ps.queue[t->iteration & 1] + sq->base;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-    const int pid = qin[q];
-    resolve_path(sc, t->fp[ps.seg[pid]], ps, pid, capacity);
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int q = base + threadIdx.x;
+    if (q < n) {
+      const int pid = qin[q];
+      resolve_path(sc, t->fp[ps.seg[pid]], ps, pid, capacity);
+    }
+    __syncwarp();
   }
 }
 

@@ -29,10 +29,17 @@ namespace mcrt {
 
 namespace {
 
-constexpr int kBins = 16;      // bvh.ts:3
+constexpr int kBins = 16;      // bvh.ts:3 (the default; a build may ask for up to kMaxBins)
+constexpr int kMaxBins = 32;
+static_assert(kBins <= kMaxBins, "the default bin count must fit the bin arrays");
 constexpr int kMaxLeaf = 4;    // bvh.ts:4
 constexpr int kBuildDepth = 100;  // bvh.ts:5
 constexpr int kBuildBlock = 256;
+// A node of at least kWideMin triangles is binned and partitioned by several
+// blocks, kSegment triangles each; the results are combined with exact
+// (order independent) atomics, so the decisions equal a single block's.
+constexpr int kWideMin = 1 << 15;
+constexpr int kSegment = 1 << 13;
 
 void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
@@ -61,9 +68,47 @@ struct Slot {
   int node, first, count, depth;
 };
 
-// mode: -1 leaf, 0 split at `bin` of `axis`, 1 split the run in half.
+// A resident mesh of instanced geometry.
+struct DMeshRef {
+  const float* pos;
+  const float* nrm;      // or nullptr: face normals
+  const float* uv;       // or nullptr: zeros
+  const uint32_t* idx;   // or nullptr: not indexed
+  int tri_count;
+};
+
+// An instance on the device: its world matrix, normal matrix (filled by
+// k_instance_matrices), first output triangle and per-triangle words.
+struct DInstance {
+  double world[16];
+  double nm[9];
+  long long tri_base;
+  int mesh, mirror, flags, side, flat;
+  uint32_t material;
+};
+
+// mode: -1 leaf, 0 split at `bin` of `axis` (binned with lo and scale), 1
+// split the run in half.
 struct Split {
   int mode, axis, bin, nleft;
+  double lo, scale;
+};
+
+// Accumulators of one wide node: bounds (node min xyz, -max xyz, centroid
+// min xyz, -max xyz, all min-reduced), then bin counts and boxes.
+struct WideAcc {
+  float box[12];
+  int cnt[3][kMaxBins];
+  float bb[3][kMaxBins][6];
+  unsigned done;
+};
+
+// Per level: blocks of each slot, where its blocks start, its wide index.
+struct LevelPlan {
+  const int* nb;     // blocks per slot
+  const int* boff;   // first block of each slot
+  const int* wid;    // index into the wide accumulators (valid when nb > 1)
+  int active;        // slots
 };
 
 // Float min / max through integer atomics (exact, order independent).
@@ -148,28 +193,66 @@ __global__ void k_prepare(const float* __restrict__ tris, int n, float4* __restr
 
 __device__ __forceinline__ float comp4(float4 v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
 
-__device__ __forceinline__ int bin_of(float c, double lo, double scale) {
-  return static_cast<int>(fmin(static_cast<double>(kBins - 1), floor((static_cast<double>(c) - lo) * scale)));
+__device__ __forceinline__ int bin_of(float c, double lo, double scale, int bins) {
+  return static_cast<int>(fmin(static_cast<double>(bins - 1), floor((static_cast<double>(c) - lo) * scale)));
 }
 
-// Bounds, leaf test, binning and SAH choice of one node per block
-// (bvh.ts:55-144).
-__global__ void __launch_bounds__(kBuildBlock) k_split(const Slot* __restrict__ slots,
-                                                       const uint32_t* __restrict__ order,
-                                                       const float4* __restrict__ bmin, const float4* __restrict__ bmax,
-                                                       const float4* __restrict__ cent, float* __restrict__ bounds,
-                                                       int* __restrict__ nodes, Split* __restrict__ split,
-                                                       int* __restrict__ is_split) {
-  const Slot s = slots[blockIdx.x];
-  const int tid = threadIdx.x;
-  __shared__ float red[kBuildBlock / 32][12];
-  __shared__ float nb[12];  // node min xyz, -max xyz, centroid min xyz, -max xyz
-  __shared__ int cnt[3][kBins];
-  __shared__ float bbox[3][kBins][6];
+// The slot whose blocks include block b: the last j with boff[j] <= b.
+__device__ __forceinline__ int slot_of_block(const LevelPlan& lp, int b) {
+  int lo = 0, hi = lp.active - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (lp.boff[mid] <= b) {
+      lo = mid;
+    } else {
+      hi = mid - 1;
+    }
+  }
+  return lo;
+}
 
+// Blocks and wide flag of each slot of a level.
+__global__ void k_level_plan(const Slot* __restrict__ slots, int active, int* __restrict__ nb,
+                             int* __restrict__ wide) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= active) return;
+  const int c = slots[j].count;
+  const int w = c >= kWideMin ? 1 : 0;
+  nb[j] = w ? (c + kSegment - 1) / kSegment : 1;
+  wide[j] = w;
+}
+
+__global__ void k_level_totals(const int* __restrict__ nb, const int* __restrict__ boff,
+                               const int* __restrict__ wide, const int* __restrict__ wid, int active,
+                               int* __restrict__ out) {
+  out[0] = boff[active - 1] + nb[active - 1];
+  out[1] = wid[active - 1] + wide[active - 1];
+}
+
+__global__ void k_wide_init(WideAcc* __restrict__ acc, int count) {
+  const int i = blockIdx.x;
+  if (i >= count) return;
+  WideAcc& a = acc[i];
+  for (int k = threadIdx.x; k < 12; k += blockDim.x) a.box[k] = INFINITY;
+  for (int k = threadIdx.x; k < 3 * kMaxBins; k += blockDim.x) {
+    const int ax = k / kMaxBins, b = k % kMaxBins;
+    a.cnt[ax][b] = 0;
+    for (int q = 0; q < 3; q++) {
+      a.bb[ax][b][q] = INFINITY;
+      a.bb[ax][b][3 + q] = -INFINITY;
+    }
+  }
+  if (threadIdx.x == 0) a.done = 0;
+}
+
+// The 12 bounds of triangles order[first, end) reduced over the block into out[12].
+__device__ void block_bounds(const uint32_t* __restrict__ order, int first, int end, const float4* __restrict__ bmin,
+                             const float4* __restrict__ bmax, const float4* __restrict__ cent, float* out) {
+  __shared__ float red[kBuildBlock / 32][12];
+  const int tid = threadIdx.x;
   float m[12];
   for (int i = 0; i < 12; i++) m[i] = INFINITY;
-  for (int k = s.first + tid; k < s.first + s.count; k += kBuildBlock) {
+  for (int k = first + tid; k < end; k += kBuildBlock) {
     const uint32_t t = order[k];
     const float4 a = bmin[t], b = bmax[t], c = cent[t];
     m[0] = fminf(m[0], a.x); m[1] = fminf(m[1], a.y); m[2] = fminf(m[2], a.z);
@@ -181,53 +264,177 @@ __global__ void __launch_bounds__(kBuildBlock) k_split(const Slot* __restrict__ 
     for (int i = 0; i < 12; i++) m[i] = fminf(m[i], __shfl_xor_sync(0xffffffffu, m[i], off));
   if ((tid & 31) == 0)
     for (int i = 0; i < 12; i++) red[tid >> 5][i] = m[i];
-  for (int i = tid; i < 3 * kBins; i += kBuildBlock) {
-    const int a = i / kBins, b = i % kBins;
-    cnt[a][b] = 0;
-    for (int j = 0; j < 3; j++) {
-      bbox[a][b][j] = INFINITY;
-      bbox[a][b][3 + j] = -INFINITY;
-    }
-  }
   __syncthreads();
   if (tid < 12) {
     float v = INFINITY;
     for (int w = 0; w < kBuildBlock / 32; w++) v = fminf(v, red[w][tid]);
-    nb[tid] = v;
+    out[tid] = v;
   }
   __syncthreads();
-  const double nx0 = nb[0], ny0 = nb[1], nz0 = nb[2], nx1 = -nb[3], ny1 = -nb[4], nz1 = -nb[5];
-  const double cmin[3] = {nb[6], nb[7], nb[8]};
-  const double cmax[3] = {-nb[9], -nb[10], -nb[11]};
-  if (tid == 0) {
+}
+
+// Partial bounds of each wide node, one segment per block.
+__global__ void __launch_bounds__(kBuildBlock) k_bounds(LevelPlan lp, const Slot* __restrict__ slots,
+                                                        const uint32_t* __restrict__ order,
+                                                        const float4* __restrict__ bmin,
+                                                        const float4* __restrict__ bmax,
+                                                        const float4* __restrict__ cent, WideAcc* __restrict__ acc) {
+  __shared__ int sj;
+  if (threadIdx.x == 0) sj = slot_of_block(lp, blockIdx.x);
+  __syncthreads();
+  const int j = sj;
+  if (lp.nb[j] <= 1) return;
+  const Slot s = slots[j];
+  const int seg = blockIdx.x - lp.boff[j];
+  const int first = s.first + seg * kSegment;
+  const int end = min(s.first + s.count, first + kSegment);
+  __shared__ float part[12];
+  block_bounds(order, first, end, bmin, bmax, cent, part);
+  if (threadIdx.x < 12) atomic_min_f(&acc[lp.wid[j]].box[threadIdx.x], part[threadIdx.x]);
+}
+
+// The SAH sweeps (bvh.ts:110-134) and the choice (bvh.ts:137-163) of one
+// node from its bins, on one thread. nb: the node's 12 bounds as block_bounds
+// gives them; lo / scale / live: the binning of each axis.
+__device__ void decide(const Slot& s, const float* nb, const int (*cnt)[kMaxBins], const float (*bbox)[kMaxBins][6],
+                       const double* lo, const double* scale, const bool* live, int bins, int j, int* nodes,
+                       Split* split, int* is_split) {
+  double best_cost = INFINITY;
+  int best_axis = -1, best_split = -1;
+  double right_area[kMaxBins];
+  int right_count[kMaxBins];
+  for (int a = 0; a < 3; a++) {
+    if (!live[a]) continue;
+    double rx0 = INFINITY, ry0 = INFINITY, rz0 = INFINITY, rx1 = -INFINITY, ry1 = -INFINITY, rz1 = -INFINITY;
+    int rc = 0;
+    for (int i = bins - 1; i > 0; i--) {
+      const float* o = bbox[a][i];
+      rc += cnt[a][i];
+      rx0 = fmin(rx0, static_cast<double>(o[0])); ry0 = fmin(ry0, static_cast<double>(o[1]));
+      rz0 = fmin(rz0, static_cast<double>(o[2]));
+      rx1 = fmax(rx1, static_cast<double>(o[3])); ry1 = fmax(ry1, static_cast<double>(o[4]));
+      rz1 = fmax(rz1, static_cast<double>(o[5]));
+      right_count[i] = rc;
+      right_area[i] = rc > 0 ? area(rx0, ry0, rz0, rx1, ry1, rz1) : 0;
+    }
+    double lx0 = INFINITY, ly0 = INFINITY, lz0 = INFINITY, lx1 = -INFINITY, ly1 = -INFINITY, lz1 = -INFINITY;
+    int lc = 0;
+    for (int i = 0; i < bins - 1; i++) {
+      const float* o = bbox[a][i];
+      lc += cnt[a][i];
+      lx0 = fmin(lx0, static_cast<double>(o[0])); ly0 = fmin(ly0, static_cast<double>(o[1]));
+      lz0 = fmin(lz0, static_cast<double>(o[2]));
+      lx1 = fmax(lx1, static_cast<double>(o[3])); ly1 = fmax(ly1, static_cast<double>(o[4]));
+      lz1 = fmax(lz1, static_cast<double>(o[5]));
+      const int rc2 = right_count[i + 1];
+      if (lc == 0 || rc2 == 0) continue;
+      const double cost = lc * area(lx0, ly0, lz0, lx1, ly1, lz1) + rc2 * right_area[i + 1];
+      if (cost < best_cost) {
+        best_cost = cost;
+        best_axis = a;
+        best_split = i;
+      }
+    }
+  }
+  Split d{1, 0, 0, s.count >> 1, 0.0, 0.0};
+  bool leaf = false;
+  if (best_axis >= 0) {
+    const double parent_area = area(nb[0], nb[1], nb[2], -static_cast<double>(nb[3]), -static_cast<double>(nb[4]),
+                                     -static_cast<double>(nb[5]));
+    const double split_cost = 1 + (1 * best_cost) / fmax(parent_area, 1e-30);
+    if (split_cost >= 1.0 * s.count && s.count <= 16) {
+      leaf = true;
+    } else {
+      int nleft = 0;
+      for (int i = 0; i <= best_split; i++) nleft += cnt[best_axis][i];
+      d = Split{0, best_axis, best_split, nleft, lo[best_axis], scale[best_axis]};
+      if (nleft == 0 || nleft == s.count) d = Split{1, best_axis, 0, s.count >> 1, 0.0, 0.0};
+    }
+  }
+  if (leaf) {
+    int* nd = nodes + 3 * static_cast<size_t>(s.node);
+    nd[0] = s.first; nd[1] = s.count; nd[2] = 0;
+    split[j] = Split{-1, 0, 0, 0, 0.0, 0.0};
+    is_split[j] = 0;
+  } else {
+    split[j] = d;
+    is_split[j] = 1;
+  }
+}
+
+// Bounds, leaf test, binning and SAH choice of every node of a level
+// (bvh.ts:55-144). A node of one block is handled by that block alone; the
+// blocks of a wide node bin their segments into the node's accumulators
+// (k_bounds has reduced its bounds) and the last block to finish decides.
+__global__ void __launch_bounds__(kBuildBlock) k_split(LevelPlan lp, const Slot* __restrict__ slots,
+                                                       const uint32_t* __restrict__ order,
+                                                       const float4* __restrict__ bmin, const float4* __restrict__ bmax,
+                                                       const float4* __restrict__ cent, float* __restrict__ bounds,
+                                                       int* __restrict__ nodes, Split* __restrict__ split,
+                                                       int* __restrict__ is_split, WideAcc* __restrict__ acc,
+                                                       int bins) {
+  __shared__ int sj;
+  __shared__ float nb[12];  // node min xyz, -max xyz, centroid min xyz, -max xyz
+  __shared__ int cnt[3][kMaxBins];
+  __shared__ float bbox[3][kMaxBins][6];
+  __shared__ int last;
+  const int tid = threadIdx.x;
+  if (tid == 0) sj = slot_of_block(lp, blockIdx.x);
+  __syncthreads();
+  const int j = sj;
+  const Slot s = slots[j];
+  const int blocks = lp.nb[j];
+  const bool wide = blocks > 1;
+  const int seg = blockIdx.x - lp.boff[j];
+  WideAcc* wa = wide ? acc + lp.wid[j] : nullptr;
+  if (wide) {
+    if (tid < 12) nb[tid] = __ldcg(&wa->box[tid]);
+    __syncthreads();
+  } else {
+    block_bounds(order, s.first, s.first + s.count, bmin, bmax, cent, nb);
+  }
+  if (tid == 0 && seg == 0) {
     float* bo = bounds + 6 * static_cast<size_t>(s.node);
     bo[0] = nb[0]; bo[1] = nb[1]; bo[2] = nb[2];
     bo[3] = -nb[3]; bo[4] = -nb[4]; bo[5] = -nb[5];
   }
   if (s.count <= kMaxLeaf || s.depth >= kBuildDepth) {
-    if (tid == 0) {
+    if (tid == 0 && seg == 0) {
       int* nd = nodes + 3 * static_cast<size_t>(s.node);
       nd[0] = s.first; nd[1] = s.count; nd[2] = 0;
-      split[blockIdx.x] = Split{-1, 0, 0, 0};
-      is_split[blockIdx.x] = 0;
+      split[j] = Split{-1, 0, 0, 0, 0.0, 0.0};
+      is_split[j] = 0;
     }
     return;
   }
+  for (int i = tid; i < 3 * kMaxBins; i += kBuildBlock) {
+    const int a = i / kMaxBins, b = i % kMaxBins;
+    cnt[a][b] = 0;
+    for (int q = 0; q < 3; q++) {
+      bbox[a][b][q] = INFINITY;
+      bbox[a][b][3 + q] = -INFINITY;
+    }
+  }
   // Bin the centroids along every axis with extent (bvh.ts:89-109).
+  const double cmin[3] = {nb[6], nb[7], nb[8]};
+  const double cmax[3] = {-nb[9], -nb[10], -nb[11]};
   double lo[3], scale[3];
   bool live[3];
   for (int a = 0; a < 3; a++) {
     lo[a] = cmin[a];
     const double extent = cmax[a] - lo[a];
     live[a] = extent > 0;
-    scale[a] = live[a] ? kBins / extent : 0.0;
+    scale[a] = live[a] ? bins / extent : 0.0;
   }
-  for (int k = s.first + tid; k < s.first + s.count; k += kBuildBlock) {
+  __syncthreads();
+  const int first = wide ? s.first + seg * kSegment : s.first;
+  const int end = wide ? min(s.first + s.count, first + kSegment) : s.first + s.count;
+  for (int k = first + tid; k < end; k += kBuildBlock) {
     const uint32_t t = order[k];
     const float4 a4 = bmin[t], b4 = bmax[t], c4 = cent[t];
     for (int a = 0; a < 3; a++) {
       if (!live[a]) continue;
-      const int b = bin_of(comp4(c4, a), lo[a], scale[a]);
+      const int b = bin_of(comp4(c4, a), lo[a], scale[a], bins);
       atomicAdd(&cnt[a][b], 1);
       atomic_min_f(&bbox[a][b][0], a4.x);
       atomic_min_f(&bbox[a][b][1], a4.y);
@@ -238,148 +445,134 @@ __global__ void __launch_bounds__(kBuildBlock) k_split(const Slot* __restrict__ 
     }
   }
   __syncthreads();
+  if (wide) {
+    // Fold this segment's bins into the node's, then let the last block decide.
+    for (int i = tid; i < 3 * bins; i += kBuildBlock) {
+      const int a = i / bins, b = i % bins;
+      if (!live[a] || cnt[a][b] == 0) continue;
+      atomicAdd(&wa->cnt[a][b], cnt[a][b]);
+      for (int q = 0; q < 3; q++) {
+        atomic_min_f(&wa->bb[a][b][q], bbox[a][b][q]);
+        atomic_max_f(&wa->bb[a][b][3 + q], bbox[a][b][3 + q]);
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) last = atomicAdd(&wa->done, 1u) == static_cast<unsigned>(blocks - 1) ? 1 : 0;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int i = tid; i < 3 * bins; i += kBuildBlock) {
+      const int a = i / bins, b = i % bins;
+      cnt[a][b] = __ldcg(&wa->cnt[a][b]);
+      for (int q = 0; q < 6; q++) bbox[a][b][q] = __ldcg(&wa->bb[a][b][q]);
+    }
+    __syncthreads();
+  }
+  if (tid == 0) decide(s, nb, cnt, bbox, lo, scale, live, bins, j, nodes, split, is_split);
+}
+
+// The first triangle of a block's share of its node, and the end.
+__device__ __forceinline__ void block_range(const Slot& s, bool wide, int seg, int& first, int& end) {
+  first = wide ? s.first + seg * kSegment : s.first;
+  end = wide ? min(s.first + s.count, first + kSegment) : s.first + s.count;
+}
+
+__device__ __forceinline__ int goes_left(const Split& d, const Slot& s, int k, const float4* __restrict__ cent,
+                                         const uint32_t* __restrict__ order, int bins) {
+  return d.mode == 0 ? (bin_of(comp4(cent[order[k]], d.axis), d.lo, d.scale, bins) <= d.bin ? 1 : 0)
+                     : (k - s.first < d.nleft ? 1 : 0);
+}
+
+// Triangles going left in each block's segment of a wide split node; 0 for
+// every other block.
+__global__ void __launch_bounds__(kBuildBlock) k_count_left(LevelPlan lp, const Slot* __restrict__ slots,
+                                                            const Split* __restrict__ split,
+                                                            const uint32_t* __restrict__ order,
+                                                            const float4* __restrict__ cent, int bins,
+                                                            int* __restrict__ blk_left) {
+  __shared__ int sj;
+  __shared__ int part[kBuildBlock / 32];
+  const int tid = threadIdx.x;
+  if (tid == 0) sj = slot_of_block(lp, blockIdx.x);
+  __syncthreads();
+  const int j = sj;
+  const Split d = split[j];
+  if (lp.nb[j] <= 1 || d.mode < 0) {
+    if (tid == 0) blk_left[blockIdx.x] = 0;
+    return;
+  }
+  const Slot s = slots[j];
+  int first, end;
+  block_range(s, true, blockIdx.x - lp.boff[j], first, end);
+  int c = 0;
+  for (int k = first + tid; k < end; k += kBuildBlock) c += goes_left(d, s, k, cent, order, bins);
+  for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+  if ((tid & 31) == 0) part[tid >> 5] = c;
+  __syncthreads();
   if (tid == 0) {
-    // SAH sweeps, bvh.ts:110-134, and the choice, bvh.ts:137-163.
-    double best_cost = INFINITY;
-    int best_axis = -1, best_split = -1;
-    double right_area[kBins];
-    int right_count[kBins];
-    for (int a = 0; a < 3; a++) {
-      if (!live[a]) continue;
-      double rx0 = INFINITY, ry0 = INFINITY, rz0 = INFINITY, rx1 = -INFINITY, ry1 = -INFINITY, rz1 = -INFINITY;
-      int rc = 0;
-      for (int i = kBins - 1; i > 0; i--) {
-        const float* o = bbox[a][i];
-        rc += cnt[a][i];
-        rx0 = fmin(rx0, static_cast<double>(o[0])); ry0 = fmin(ry0, static_cast<double>(o[1]));
-        rz0 = fmin(rz0, static_cast<double>(o[2]));
-        rx1 = fmax(rx1, static_cast<double>(o[3])); ry1 = fmax(ry1, static_cast<double>(o[4]));
-        rz1 = fmax(rz1, static_cast<double>(o[5]));
-        right_count[i] = rc;
-        right_area[i] = rc > 0 ? area(rx0, ry0, rz0, rx1, ry1, rz1) : 0;
-      }
-      double lx0 = INFINITY, ly0 = INFINITY, lz0 = INFINITY, lx1 = -INFINITY, ly1 = -INFINITY, lz1 = -INFINITY;
-      int lc = 0;
-      for (int i = 0; i < kBins - 1; i++) {
-        const float* o = bbox[a][i];
-        lc += cnt[a][i];
-        lx0 = fmin(lx0, static_cast<double>(o[0])); ly0 = fmin(ly0, static_cast<double>(o[1]));
-        lz0 = fmin(lz0, static_cast<double>(o[2]));
-        lx1 = fmax(lx1, static_cast<double>(o[3])); ly1 = fmax(ly1, static_cast<double>(o[4]));
-        lz1 = fmax(lz1, static_cast<double>(o[5]));
-        const int rc2 = right_count[i + 1];
-        if (lc == 0 || rc2 == 0) continue;
-        const double cost = lc * area(lx0, ly0, lz0, lx1, ly1, lz1) + rc2 * right_area[i + 1];
-        if (cost < best_cost) {
-          best_cost = cost;
-          best_axis = a;
-          best_split = i;
-        }
-      }
-    }
-    Split d{1, 0, 0, s.count >> 1};
-    bool leaf = false;
-    if (best_axis >= 0) {
-      const double parent_area = area(nx0, ny0, nz0, nx1, ny1, nz1);
-      const double split_cost = 1 + (1 * best_cost) / fmax(parent_area, 1e-30);
-      if (split_cost >= 1.0 * s.count && s.count <= 16) {
-        leaf = true;
-      } else {
-        int nleft = 0;
-        for (int i = 0; i <= best_split; i++) nleft += cnt[best_axis][i];
-        d = Split{0, best_axis, best_split, nleft};
-        if (nleft == 0 || nleft == s.count) d = Split{1, best_axis, 0, s.count >> 1};
-      }
-    }
-    if (leaf) {
-      int* nd = nodes + 3 * static_cast<size_t>(s.node);
-      nd[0] = s.first; nd[1] = s.count; nd[2] = 0;
-      split[blockIdx.x] = Split{-1, 0, 0, 0};
-      is_split[blockIdx.x] = 0;
-    } else {
-      split[blockIdx.x] = d;
-      is_split[blockIdx.x] = 1;
-    }
+    int t = 0;
+    for (int w = 0; w < kBuildBlock / 32; w++) t += part[w];
+    blk_left[blockIdx.x] = t;
   }
 }
 
 // Stable partition of each split node's run and its two children
-// (bvh.ts:145-171); leaves copy their run unchanged.
-__global__ void __launch_bounds__(kBuildBlock) k_scatter(const Slot* __restrict__ slots,
+// (bvh.ts:145-171); leaves copy their run unchanged. A wide node's blocks
+// place their segments after the lefts and rights of the blocks before them
+// (blk_pre: exclusive sums of k_count_left over all blocks).
+__global__ void __launch_bounds__(kBuildBlock) k_scatter(LevelPlan lp, const Slot* __restrict__ slots,
                                                          const Split* __restrict__ split,
                                                          const int* __restrict__ rank, int child_base,
                                                          const uint32_t* __restrict__ order,
                                                          uint32_t* __restrict__ order_out,
                                                          const float4* __restrict__ cent, int* __restrict__ nodes,
-                                                         Slot* __restrict__ next) {
+                                                         Slot* __restrict__ next, const int* __restrict__ blk_pre,
+                                                         int bins) {
   using Scan = cub::BlockScan<int, kBuildBlock>;
   __shared__ typename Scan::TempStorage scan_tmp;
-  const Slot s = slots[blockIdx.x];
-  const Split d = split[blockIdx.x];
+  __shared__ int sj;
   const int tid = threadIdx.x;
-  const int end = s.first + s.count;
+  if (tid == 0) sj = slot_of_block(lp, blockIdx.x);
+  __syncthreads();
+  const int j = sj;
+  const Slot s = slots[j];
+  const Split d = split[j];
+  const bool wide = lp.nb[j] > 1;
+  const int seg = blockIdx.x - lp.boff[j];
+  int first, end;
+  block_range(s, wide, seg, first, end);
   if (d.mode < 0) {
-    for (int k = s.first + tid; k < end; k += kBuildBlock) order_out[k] = order[k];
+    for (int k = first + tid; k < end; k += kBuildBlock) order_out[k] = order[k];
     return;
   }
-  double lo = 0, scale = 0;
-  if (d.mode == 0) {
-    // The same bins as k_split: recompute the centroid range along the axis.
-    float mn = INFINITY, mx = -INFINITY;
-    for (int k = s.first + tid; k < end; k += kBuildBlock) {
-      const float c = comp4(cent[order[k]], d.axis);
-      mn = fminf(mn, c);
-      mx = fmaxf(mx, c);
-    }
-    __shared__ float rmn[kBuildBlock / 32], rmx[kBuildBlock / 32];
-    __shared__ float fmn, fmx;
-    for (int off = 16; off > 0; off >>= 1) {
-      mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, off));
-      mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-    }
-    if ((tid & 31) == 0) {
-      rmn[tid >> 5] = mn;
-      rmx[tid >> 5] = mx;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      float a = INFINITY, b = -INFINITY;
-      for (int w = 0; w < kBuildBlock / 32; w++) {
-        a = fminf(a, rmn[w]);
-        b = fmaxf(b, rmx[w]);
-      }
-      fmn = a;
-      fmx = b;
-    }
-    __syncthreads();
-    lo = fmn;
-    scale = kBins / (static_cast<double>(fmx) - lo);
-  }
-  int left_off = 0;
-  for (int base = s.first; base < end; base += kBuildBlock) {
+  int left_off = wide ? blk_pre[blockIdx.x] - blk_pre[lp.boff[j]] : 0;
+  int right_off = (first - s.first) - left_off;
+  for (int base = first; base < end; base += kBuildBlock) {
     const int k = base + tid;
     int f = 0;
     uint32_t t = 0;
     if (k < end) {
       t = order[k];
-      f = d.mode == 0 ? (bin_of(comp4(cent[t], d.axis), lo, scale) <= d.bin ? 1 : 0) : (k - s.first < d.nleft ? 1 : 0);
+      f = goes_left(d, s, k, cent, order, bins);
     }
     int pre = 0, total = 0;
     Scan(scan_tmp).ExclusiveSum(f, pre, total);
     if (k < end) {
-      const int right_before = (base - s.first) - left_off;
-      const int dst = f ? s.first + left_off + pre : s.first + d.nleft + right_before + (tid - pre);
+      const int dst = f ? s.first + left_off + pre : s.first + d.nleft + right_off + (tid - pre);
       order_out[dst] = t;
     }
+    const int in_chunk = min(kBuildBlock, end - base);
     left_off += total;
+    right_off += in_chunk - total;
     __syncthreads();
   }
-  if (tid == 0) {
-    const int left = child_base + 2 * rank[blockIdx.x];
+  if (tid == 0 && seg == 0) {
+    const int left = child_base + 2 * rank[j];
     int* nd = nodes + 3 * static_cast<size_t>(s.node);
     nd[0] = left; nd[1] = 0; nd[2] = d.axis;
-    next[2 * rank[blockIdx.x]] = Slot{left, s.first, d.nleft, s.depth + 1};
-    next[2 * rank[blockIdx.x] + 1] = Slot{left + 1, s.first + d.nleft, s.count - d.nleft, s.depth + 1};
+    next[2 * rank[j]] = Slot{left, s.first, d.nleft, s.depth + 1};
+    next[2 * rank[j] + 1] = Slot{left + 1, s.first + d.nleft, s.count - d.nleft, s.depth + 1};
   }
 }
 
@@ -486,6 +679,124 @@ __global__ void k_tangents(const float* __restrict__ tris, const float* __restri
 
 int blocks_of(long long n, int b) { return static_cast<int>((n + b - 1) / b); }
 
+// ---- instanced geometry on the device (addMesh, src/compile.ts:212-306)
+
+// normalMatrix, src/compile.ts:192-205: cofactors divided by the determinant,
+// evaluated in the reference's order (this file is compiled without FMA).
+__global__ void k_instance_matrices(DInstance* __restrict__ inst, int count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  DInstance& d = inst[i];
+  const double* m = d.world;
+  const double a = m[0], b = m[4], c = m[8], dd = m[1], e = m[5], f = m[9], g = m[2], h = m[6], ii = m[10];
+  const double A = e * ii - f * h, B = -(dd * ii - f * g), C = dd * h - e * g;
+  const double det = a * A + b * B + c * C;
+  const double sc = det != 0 ? 1 / det : 0;
+  d.nm[0] = A * sc; d.nm[1] = (-(b * ii - c * h)) * sc; d.nm[2] = (b * f - c * e) * sc;
+  d.nm[3] = B * sc; d.nm[4] = (a * ii - c * g) * sc; d.nm[5] = (-(a * f - c * dd)) * sc;
+  d.nm[6] = C * sc; d.nm[7] = (-(a * h - b * g)) * sc; d.nm[8] = (a * e - b * dd) * sc;
+  d.mirror = det < 0 ? 1 : 0;
+}
+
+// One thread per triangle of instance blockIdx.y: world-space positions in
+// double, float32 v0 / e1 / e2 as the compile's Float32Array stores make them
+// (compile.ts:337-343), normals through the normal matrix normalised with
+// Math.hypot (or the face normal), uvs, material, flags, side; and the
+// largest coordinate for the epsilon.
+__global__ void k_flatten(const DInstance* __restrict__ inst, const DMeshRef* __restrict__ meshes,
+                          float* __restrict__ tris, float* __restrict__ nrm, float* __restrict__ uvs,
+                          uint32_t* __restrict__ mats, uint8_t* __restrict__ flags, uint8_t* __restrict__ sides,
+                          unsigned long long* __restrict__ max_coord) {
+  const DInstance& d = inst[blockIdx.y];
+  const DMeshRef mr = meshes[d.mesh];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  double mc = 0;
+  if (k < mr.tri_count) {
+    const size_t o = static_cast<size_t>(d.tri_base) + k;
+    int ids[3] = {3 * k, 3 * k + 1, 3 * k + 2};
+    if (mr.idx) {
+      for (int v = 0; v < 3; v++) ids[v] = static_cast<int>(mr.idx[ids[v]]);
+    }
+    if (d.mirror) {  // a mirroring transform reverses the winding
+      const int t = ids[1];
+      ids[1] = ids[2];
+      ids[2] = t;
+    }
+    const double* w = d.world;
+    double p[9];
+    for (int v = 0; v < 3; v++) {
+      const float* q = mr.pos + 3 * static_cast<size_t>(ids[v]);
+      const double x = q[0], y = q[1], z = q[2];
+      p[3 * v] = w[0] * x + w[4] * y + w[8] * z + w[12];
+      p[3 * v + 1] = w[1] * x + w[5] * y + w[9] * z + w[13];
+      p[3 * v + 2] = w[2] * x + w[6] * y + w[10] * z + w[14];
+    }
+    float* t = tris + 9 * o;
+    for (int a = 0; a < 3; a++) {
+      t[a] = static_cast<float>(p[a]);
+      t[3 + a] = static_cast<float>(p[3 + a] - p[a]);
+      t[6 + a] = static_cast<float>(p[6 + a] - p[a]);
+    }
+    for (int q = 0; q < 9; q++) mc = fmax(mc, fabs(p[q]));
+    float* nn = nrm + 9 * o;
+    if (mr.nrm && !d.flat) {
+      for (int v = 0; v < 3; v++) {
+        const float* q = mr.nrm + 3 * static_cast<size_t>(ids[v]);
+        const double x = q[0], y = q[1], z = q[2];
+        const double nx = d.nm[0] * x + d.nm[3] * y + d.nm[6] * z;
+        const double ny = d.nm[1] * x + d.nm[4] * y + d.nm[7] * z;
+        const double nz = d.nm[2] * x + d.nm[5] * y + d.nm[8] * z;
+        double len = js_hypot3(nx, ny, nz);
+        if (!(len != 0) || isnan(len)) len = 1;  // Math.hypot(...) || 1
+        nn[3 * v] = static_cast<float>(nx / len);
+        nn[3 * v + 1] = static_cast<float>(ny / len);
+        nn[3 * v + 2] = static_cast<float>(nz / len);
+      }
+    } else {
+      const double ex = p[3] - p[0], ey = p[4] - p[1], ez = p[5] - p[2];
+      const double fx = p[6] - p[0], fy = p[7] - p[1], fz = p[8] - p[2];
+      const double cx = ey * fz - ez * fy, cy = ez * fx - ex * fz, cz = ex * fy - ey * fx;
+      const double len = js_hypot3(cx, cy, cz);
+      float f3[3] = {0.0f, 0.0f, 1.0f};
+      if (len > 0) {
+        f3[0] = static_cast<float>(cx / len);
+        f3[1] = static_cast<float>(cy / len);
+        f3[2] = static_cast<float>(cz / len);
+      }
+      for (int v = 0; v < 3; v++)
+        for (int a = 0; a < 3; a++) nn[3 * v + a] = f3[a];
+    }
+    float* u = uvs + 6 * o;
+    for (int v = 0; v < 3; v++) {
+      u[2 * v] = mr.uv ? mr.uv[2 * static_cast<size_t>(ids[v])] : 0.0f;
+      u[2 * v + 1] = mr.uv ? mr.uv[2 * static_cast<size_t>(ids[v]) + 1] : 0.0f;
+    }
+    mats[o] = d.material;
+    flags[o] = static_cast<uint8_t>(d.flags);
+    sides[o] = static_cast<uint8_t>(d.side);
+  }
+  for (int off = 16; off > 0; off >>= 1) mc = fmax(mc, __shfl_xor_sync(0xffffffffu, mc, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(max_coord, static_cast<unsigned long long>(__double_as_longlong(mc)));
+}
+
+// Float32 arrays into BVH order (compile.ts:364-377, the float path).
+__global__ void k_reorder_f32(const uint32_t* __restrict__ order, int n, const float* __restrict__ tris_in,
+                              const float* __restrict__ nrm, const float* __restrict__ uv,
+                              const uint32_t* __restrict__ mats, const uint8_t* __restrict__ flags,
+                              const uint8_t* __restrict__ sides, float* __restrict__ tris_out,
+                              float* __restrict__ nrm_out, float* __restrict__ uv_out, uint32_t* __restrict__ mats_out,
+                              uint8_t* __restrict__ flags_out, uint8_t* __restrict__ sides_out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t s = order[i];
+  for (int k = 0; k < 9; k++) tris_out[9 * static_cast<size_t>(i) + k] = tris_in[9 * s + k];
+  for (int k = 0; k < 9; k++) nrm_out[9 * static_cast<size_t>(i) + k] = nrm[9 * s + k];
+  for (int k = 0; k < 6; k++) uv_out[6 * static_cast<size_t>(i) + k] = uv[6 * s + k];
+  mats_out[i] = mats[s];
+  flags_out[i] = flags[s];
+  sides_out[i] = sides[s];
+}
+
 }  // namespace
 
 struct BuildBuffers {
@@ -494,6 +805,8 @@ struct BuildBuffers {
   DevArray<Slot> slots[2];
   DevArray<Split> split;
   DevArray<int> is_split, rank;
+  DevArray<int> nb, boff, wide, wid, blk_left, blk_pre, totals;
+  DevArray<WideAcc> acc;
   DevArray<uint8_t> scan_tmp;
   DevArray<int> host_pair;
   // compile
@@ -503,42 +816,77 @@ struct BuildBuffers {
   DevArray<float> tris, tris_out, nrm_out, uv_out, col_out, tan_out, bounds;
   DevArray<int> nodes;
   DevArray<unsigned long long> max_coord;
+  // instanced geometry
+  DevArray<DInstance> inst;
+  DevArray<DMeshRef> mesh_refs;
+  DevArray<float> flat_nrm, flat_uv;
+  std::vector<DevArray<float>> mesh_pos, mesh_nrm, mesh_uv;
+  std::vector<DevArray<uint32_t>> mesh_idx;
+  std::vector<int> mesh_tris;
 };
 
 SceneBuilder::SceneBuilder() : b_(new BuildBuffers()) {}
 SceneBuilder::~SceneBuilder() { delete b_; }
 
 int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int* d_nodes, uint32_t* d_order,
-                               cudaStream_t s) {
+                               cudaStream_t s, int bins) {
   last_levels_ = 0;
   if (n <= 0) return 0;
+  if (bins < 2 || bins > kMaxBins) throw std::runtime_error("bin count out of range");
   BuildBuffers& B = *b_;
   float4* bmin = B.bmin.ensure(n);
   float4* bmax = B.bmax.ensure(n);
   float4* cent = B.cent.ensure(n);
   uint32_t* tmp = B.order_tmp.ensure(n);
   const int max_slots = std::max(1, n);
+  // Blocks of a level: one per node, plus the extra segments of wide nodes.
+  const int max_blocks = max_slots + n / kSegment + 1;
   Slot* slots[2] = {B.slots[0].ensure(max_slots), B.slots[1].ensure(max_slots)};
   Split* split = B.split.ensure(max_slots);
   int* is_split = B.is_split.ensure(max_slots);
   int* rank = B.rank.ensure(max_slots);
+  int* nbk = B.nb.ensure(max_slots);
+  int* boff = B.boff.ensure(max_slots);
+  int* wide = B.wide.ensure(max_slots);
+  int* wid = B.wid.ensure(max_slots);
+  int* blk_left = B.blk_left.ensure(max_blocks);
+  int* blk_pre = B.blk_pre.ensure(max_blocks);
+  int* totals = B.totals.ensure(2);
+  WideAcc* acc = B.acc.ensure(n / kWideMin + 1);
   k_prepare<<<blocks_of(n, 256), 256, 0, s>>>(d_tris, n, bmin, bmax, cent, d_order);
   Slot root{0, 0, n, 0};
   check(cudaMemcpyAsync(slots[0], &root, sizeof(Slot), cudaMemcpyHostToDevice, s), "upload");
   size_t scan_bytes = 0;
-  check(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, is_split, rank, max_slots, s), "scan");
+  check(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, blk_left, blk_pre, max_blocks, s), "scan");
   uint8_t* scan_tmp = B.scan_tmp.ensure(scan_bytes);
   int active = 1, total = 1, cur = 0;
   uint32_t* order_a = d_order;
   uint32_t* order_b = tmp;
-  int pair[2];
+  int pair[2], tot[2];
   while (active > 0) {
-    k_split<<<active, kBuildBlock, 0, s>>>(slots[cur], order_a, bmin, bmax, cent, d_bounds, d_nodes, split, is_split);
+    k_level_plan<<<blocks_of(active, 256), 256, 0, s>>>(slots[cur], active, nbk, wide);
+    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, nbk, boff, active, s), "scan");
+    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, wide, wid, active, s), "scan");
+    k_level_totals<<<1, 1, 0, s>>>(nbk, boff, wide, wid, active, totals);
+    check(cudaMemcpyAsync(tot, totals, sizeof(tot), cudaMemcpyDeviceToHost, s), "download");
+    check(cudaStreamSynchronize(s), "BVH level plan");
+    const int nblocks = tot[0], nwide = tot[1];
+    const LevelPlan lp{nbk, boff, wid, active};
+    if (nwide > 0) {
+      k_wide_init<<<nwide, 128, 0, s>>>(acc, nwide);
+      k_bounds<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], order_a, bmin, bmax, cent, acc);
+    }
+    k_split<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], order_a, bmin, bmax, cent, d_bounds, d_nodes, split,
+                                            is_split, acc, bins);
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, is_split, rank, active, s), "scan");
     check(cudaMemcpyAsync(&pair[0], rank + active - 1, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
     check(cudaMemcpyAsync(&pair[1], is_split + active - 1, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
-    k_scatter<<<active, kBuildBlock, 0, s>>>(slots[cur], split, rank, total, order_a, order_b, cent, d_nodes,
-                                             slots[cur ^ 1]);
+    if (nwide > 0) {
+      k_count_left<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], split, order_a, cent, bins, blk_left);
+      check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, blk_left, blk_pre, nblocks, s), "scan");
+    }
+    k_scatter<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], split, rank, total, order_a, order_b, cent, d_nodes,
+                                              slots[cur ^ 1], blk_pre, bins);
     check(cudaStreamSynchronize(s), "BVH level");
     const int splits = pair[0] + pair[1];
     std::swap(order_a, order_b);
@@ -553,6 +901,175 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
   check(cudaGetLastError(), "BVH build");
   check(cudaStreamSynchronize(s), "BVH build");
   return total;
+}
+
+void SceneBuilder::upload_meshes(int count, const MeshInput* meshes, cudaStream_t s) {
+  BuildBuffers& B = *b_;
+  B.mesh_pos.clear();
+  B.mesh_nrm.clear();
+  B.mesh_uv.clear();
+  B.mesh_idx.clear();
+  B.mesh_tris.assign(count, 0);
+  B.mesh_pos.resize(count);
+  B.mesh_nrm.resize(count);
+  B.mesh_uv.resize(count);
+  B.mesh_idx.resize(count);
+  std::vector<DMeshRef> refs(std::max(count, 1));
+  auto up = [&](void* d, const void* h, size_t bytes) {
+    check(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s), "upload");
+  };
+  for (int i = 0; i < count; i++) {
+    const MeshInput& m = meshes[i];
+    const size_t v = static_cast<size_t>(m.vertex_count);
+    DMeshRef r{};
+    r.pos = B.mesh_pos[i].ensure(3 * v);
+    up(const_cast<float*>(r.pos), m.position, sizeof(float) * 3 * v);
+    if (m.normal) {
+      r.nrm = B.mesh_nrm[i].ensure(3 * v);
+      up(const_cast<float*>(r.nrm), m.normal, sizeof(float) * 3 * v);
+    }
+    if (m.uv) {
+      r.uv = B.mesh_uv[i].ensure(2 * v);
+      up(const_cast<float*>(r.uv), m.uv, sizeof(float) * 2 * v);
+    }
+    if (m.index_count > 0) {
+      r.idx = B.mesh_idx[i].ensure(static_cast<size_t>(m.index_count));
+      up(const_cast<uint32_t*>(r.idx), m.index, sizeof(uint32_t) * m.index_count);
+    }
+    r.tri_count = (m.index_count > 0 ? m.index_count : m.vertex_count) / 3;
+    B.mesh_tris[i] = r.tri_count;
+    refs[i] = r;
+  }
+  DMeshRef* d_refs = B.mesh_refs.ensure(refs.size());
+  up(d_refs, refs.data(), sizeof(DMeshRef) * refs.size());
+  check(cudaStreamSynchronize(s), "mesh upload");
+}
+
+long long SceneBuilder::instance_triangles(int count, const InstanceInput* inst) const {
+  long long n = 0;
+  for (int i = 0; i < count; i++) {
+    const int m = inst[i].mesh;
+    if (m < 0 || m >= static_cast<int>(b_->mesh_tris.size())) return -1;
+    n += b_->mesh_tris[m];
+  }
+  return n;
+}
+
+void SceneBuilder::compile_instances(int count, const InstanceInput* inst, int bins, cudaStream_t s,
+                                     DeviceGeometry* out, float* times_ms) {
+  BuildBuffers& B = *b_;
+  const long long total = instance_triangles(count, inst);
+  if (total < 0) throw std::runtime_error("an instance names a mesh that was not uploaded");
+  if (total > (1ll << 30)) throw std::runtime_error("too many triangles");
+  const int n = static_cast<int>(total);
+  const size_t N = static_cast<size_t>(std::max(n, 1));
+  const size_t cap = std::max<size_t>(1, 2 * N - 1);
+  cudaEvent_t ev[4];
+  for (auto& e : ev) check(cudaEventCreate(&e), "event");
+  check(cudaEventRecord(ev[0], s), "event");
+  // Instance table: tri_base and words on the host, matrices on the device.
+  std::vector<DInstance> h(std::max(count, 1));
+  long long base = 0;
+  int max_tris = 0;
+  for (int i = 0; i < count; i++) {
+    DInstance d{};
+    std::memcpy(d.world, inst[i].world, sizeof(d.world));
+    d.tri_base = base;
+    d.mesh = inst[i].mesh;
+    d.flags = inst[i].flags;
+    d.side = inst[i].side;
+    d.flat = inst[i].flat_shading;
+    d.material = inst[i].material;
+    base += B.mesh_tris[d.mesh];
+    max_tris = std::max(max_tris, B.mesh_tris[d.mesh]);
+    h[i] = d;
+  }
+  DInstance* d_inst = B.inst.ensure(h.size());
+  check(cudaMemcpyAsync(d_inst, h.data(), sizeof(DInstance) * h.size(), cudaMemcpyHostToDevice, s), "upload");
+  k_instance_matrices<<<blocks_of(count, 128), 128, 0, s>>>(d_inst, count);
+  float* d_tris = B.tris.ensure(9 * N);
+  float* d_n = B.flat_nrm.ensure(9 * N);
+  float* d_uv = B.flat_uv.ensure(6 * N);
+  uint32_t* d_m = B.mats.ensure(N);
+  uint8_t* d_f = B.flags.ensure(N);
+  uint8_t* d_s = B.sides.ensure(N);
+  unsigned long long* d_mc = B.max_coord.ensure(1);
+  check(cudaMemsetAsync(d_mc, 0, sizeof(unsigned long long), s), "memset");
+  if (count > 0 && max_tris > 0) {
+    const dim3 grid(blocks_of(max_tris, 256), count);
+    k_flatten<<<grid, 256, 0, s>>>(d_inst, B.mesh_refs.p, d_tris, d_n, d_uv, d_m, d_f, d_s, d_mc);
+  }
+  check(cudaGetLastError(), "flatten");
+  check(cudaEventRecord(ev[1], s), "event");
+  float* d_bounds = B.bounds.ensure(6 * cap);
+  int* d_nodes = B.nodes.ensure(3 * cap);
+  uint32_t* d_order = B.order.ensure(N);
+  const int m = build_device(d_tris, n, d_bounds, d_nodes, d_order, s, bins);
+  check(cudaEventRecord(ev[2], s), "event");
+  float* t_out = B.tris_out.ensure(9 * N);
+  float* n_out = B.nrm_out.ensure(9 * N);
+  float* uv_out = B.uv_out.ensure(6 * N);
+  float* tg_out = B.tan_out.ensure(4 * N);
+  uint32_t* m_out = B.mats_out.ensure(N);
+  uint8_t* f_out = B.flags_out.ensure(N);
+  uint8_t* s_out = B.sides_out.ensure(N);
+  double box_init[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  double* d_box = B.box.ensure(6);
+  check(cudaMemcpyAsync(d_box, box_init, sizeof(box_init), cudaMemcpyHostToDevice, s), "upload");
+  if (n > 0) {
+    k_reorder_f32<<<blocks_of(n, 256), 256, 0, s>>>(d_order, n, d_tris, d_n, d_uv, d_m, d_f, d_s, t_out, n_out,
+                                                    uv_out, m_out, f_out, s_out);
+    k_tangents<<<blocks_of(n, 256), 256, 0, s>>>(t_out, uv_out, n, tg_out, d_box);
+  }
+  check(cudaGetLastError(), "compile");
+  double box[6];
+  unsigned long long mc_bits = 0;
+  check(cudaMemcpyAsync(box, d_box, sizeof(box), cudaMemcpyDeviceToHost, s), "download");
+  check(cudaMemcpyAsync(&mc_bits, d_mc, sizeof(mc_bits), cudaMemcpyDeviceToHost, s), "download");
+  int root[3] = {0, 0, 0};
+  if (m > 0) check(cudaMemcpyAsync(root, d_nodes, sizeof(root), cudaMemcpyDeviceToHost, s), "download");
+  check(cudaEventRecord(ev[3], s), "event");
+  check(cudaStreamSynchronize(s), "compile");
+  double max_coordinate;
+  std::memcpy(&max_coordinate, &mc_bits, sizeof(double));
+  const double diagonal = n > 0 ? js_hypot3(box[3] - box[0], box[4] - box[1], box[5] - box[2]) : 1.0;
+  if (times_ms) {
+    for (int i = 0; i < 3; i++) cudaEventElapsedTime(&times_ms[i], ev[i], ev[i + 1]);
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  DeviceGeometry g{};
+  g.n = n;
+  g.node_count = m;
+  g.root_count = (m > 0 && root[1] > 0) ? root[1] : 0;
+  g.epsilon = n > 0 ? std::max(diagonal * 1e-5, std::max(max_coordinate * 2e-6, 1e-7)) : std::max(1e-5, 1e-7);
+  g.triangles = t_out;
+  g.normals = n_out;
+  g.uvs = uv_out;
+  g.tangents = tg_out;
+  g.materials = m_out;
+  g.flags = f_out;
+  g.sides = s_out;
+  g.bounds = d_bounds;
+  g.nodes = d_nodes;
+  g.order = d_order;
+  g.levels = last_levels_;
+  *out = g;
+}
+
+size_t SceneBuilder::device_bytes() const {
+  const BuildBuffers& B = *b_;
+  size_t t = B.bmin.n * 16 * 3 + B.order_tmp.n * 4 + (B.slots[0].n + B.slots[1].n) * sizeof(Slot) +
+             B.split.n * sizeof(Split) + (B.is_split.n + B.rank.n + B.nb.n + B.boff.n + B.wide.n + B.wid.n) * 4 +
+             (B.blk_left.n + B.blk_pre.n) * 4 + B.acc.n * sizeof(WideAcc) + B.scan_tmp.n + B.p.n * 8 + B.nrm.n * 8 +
+             B.uv.n * 8 + B.colors.n * 8 + B.tris.n * 4 + B.tris_out.n * 4 + B.nrm_out.n * 4 + B.uv_out.n * 4 +
+             B.col_out.n * 4 + B.tan_out.n * 4 + B.bounds.n * 4 + B.nodes.n * 4 + B.mats.n * 4 + B.mats_out.n * 4 +
+             B.order.n * 4 + B.flags.n + B.sides.n + B.flags_out.n + B.sides_out.n + B.has_color.n +
+             B.flat_nrm.n * 4 + B.flat_uv.n * 4 + B.inst.n * sizeof(DInstance);
+  for (const auto& a : B.mesh_pos) t += a.n * 4;
+  for (const auto& a : B.mesh_nrm) t += a.n * 4;
+  for (const auto& a : B.mesh_uv) t += a.n * 4;
+  for (const auto& a : B.mesh_idx) t += a.n * 4;
+  return t;
 }
 
 int SceneBuilder::build_bvh_host(const float* tris, int n, float* bounds, int* nodes, uint32_t* order,

@@ -206,6 +206,23 @@ class GpuExecutor:
             call("mcrt_raytrace_device", self._h, gv, sv, C.byref(cam), C.byref(st), int(width), int(height),
                  int(samples), int(bool(srgb)), C.c_void_p(device_ptr))
 
+    def raytrace_resident(self, versions: Tuple[int, int], camera: CompiledCamera, width: int, height: int,
+                          settings: TraceSettings, samples: int, srgb: bool = True,
+                          device_ptr: Optional[int] = None) -> Optional[np.ndarray]:
+        """raytraceCompiled on the geometry and shading versions this executor holds (for
+        geometry made by compile_instances): RGBA8 bytes, or into `device_ptr`."""
+        cam, st = abi.to_c_camera(camera), abi.to_c_settings(settings)
+        gv, sv = int(versions[0]), int(versions[1])
+        with self._lock:
+            if device_ptr is not None:
+                call("mcrt_raytrace_device", self._h, gv, sv, C.byref(cam), C.byref(st), int(width), int(height),
+                     int(samples), int(bool(srgb)), C.c_void_p(device_ptr))
+                return None
+            out = np.zeros(width * height * 4, np.uint8)
+            call("mcrt_raytrace", self._h, gv, sv, C.byref(cam), C.byref(st), int(width), int(height), int(samples),
+                 int(bool(srgb)), abi.ptr(out, C.c_uint8))
+            return out
+
     def render_pixels(self, scene: CompiledScene, camera: CompiledCamera, width: int, height: int,
                       settings: TraceSettings, samples: int, srgb: bool, px: np.ndarray, py: np.ndarray
                       ) -> Tuple[np.ndarray, np.ndarray]:
@@ -322,6 +339,95 @@ class GpuExecutor:
             colors=colors[: n * 12].copy() if any_colors.value else np.zeros(0, f32), materials=mats, flags=flags,
             sides=sides, bvh=CompiledBvh(bounds[: m * 6].copy(), nodes[: m * 3].copy(), m), epsilon=float(eps.value),
             order=order[:n].copy())
+
+    # ----------------------------------------------------- instanced geometry
+    def upload_meshes(self, meshes: Sequence[Any]) -> None:
+        """Meshes for compile_instances: BufferGeometry-like objects with `position` (and
+        optionally `normal`, `uv`, `index`) arrays, kept on the device."""
+        arr = (abi.mcrt_mesh * max(1, len(meshes)))()
+        keep = []
+        for i, g in enumerate(meshes):
+            pos = np.ascontiguousarray(np.asarray(g.position, np.float32).reshape(-1))
+            nrm = None if g.normal is None else np.ascontiguousarray(np.asarray(g.normal, np.float32).reshape(-1))
+            uv = None if g.uv is None else np.ascontiguousarray(np.asarray(g.uv, np.float32).reshape(-1))
+            idx = None if g.index is None else np.ascontiguousarray(np.asarray(g.index, np.uint32).reshape(-1))
+            keep += [pos, nrm, uv, idx]
+            arr[i].vertex_count = pos.size // 3
+            arr[i].index_count = 0 if idx is None else idx.size
+            arr[i].position = abi.ptr(pos, C.c_float)
+            arr[i].normal = abi.ptr(nrm, C.c_float)
+            arr[i].uv = abi.ptr(uv, C.c_float)
+            arr[i].index = abi.ptr(idx, C.c_uint32)
+        with self._lock:
+            call("mcrt_upload_meshes", self._h, len(meshes), arr)
+        self._mesh_tris = [(arr[i].index_count or arr[i].vertex_count) // 3 for i in range(len(meshes))]
+
+    def compile_instances(self, instances: Sequence[Tuple[Any, int, int, int, int, bool]], bins: int = 16,
+                          download: bool = False) -> Tuple[Dict[str, Any], Optional[CompiledGeometry]]:
+        """compileGeometry of instances of the uploaded meshes, on the GPU: each instance is
+        (world matrix [16] column-major, mesh, material, flags, side, flat_shading). The result
+        is resident (geometry version returned in the info); with `download` the compiled arrays
+        come back as a CompiledGeometry too."""
+        arr = (abi.mcrt_instance * max(1, len(instances)))()
+        for i, (world, mesh, material, flags, side, flat) in enumerate(instances):
+            w = np.asarray(world, np.float64).reshape(16)
+            for k in range(16):
+                arr[i].world[k] = float(w[k])
+            arr[i].mesh, arr[i].material = int(mesh), int(material)
+            arr[i].flags, arr[i].side, arr[i].flat_shading = int(flags), int(side), int(bool(flat))
+        self._versions += 1
+        version = self._versions
+        info = abi.mcrt_build_info()
+        out = None
+        out_c = None
+        if download:
+            n = self._instance_triangles(instances)
+            cap = max(1, 2 * n - 1)
+            f32 = np.float32
+            out = {"triangles": np.zeros(9 * n, f32), "normals": np.zeros(9 * n, f32), "uvs": np.zeros(6 * n, f32),
+                   "tangents": np.zeros(4 * n, f32), "materials": np.zeros(n, np.uint32), "flags": np.zeros(n, np.uint8),
+                   "sides": np.zeros(n, np.uint8), "bounds": np.zeros(6 * cap, f32), "nodes": np.zeros(3 * cap, np.int32),
+                   "order": np.zeros(max(1, n), np.uint32)}
+            out_c = abi.mcrt_compiled_out()
+            types = {"triangles": C.c_float, "normals": C.c_float, "uvs": C.c_float, "tangents": C.c_float,
+                     "materials": C.c_uint32, "flags": C.c_uint8, "sides": C.c_uint8, "bounds": C.c_float,
+                     "nodes": C.c_int32, "order": C.c_uint32}
+            for k, t in types.items():
+                setattr(out_c, k, abi.ptr(out[k], t))
+        with self._lock:
+            call("mcrt_compile_instances", self._h, version, len(instances), arr, int(bins), C.byref(info),
+                 C.byref(out_c) if out_c is not None else None)
+            self._geometry_version = version
+            self._scene_ref = None
+            self._geometry_ref = None
+        d = {name: getattr(info, name) for name, _ in info._fields_}
+        d["version"] = version
+        geometry = None
+        if out is not None:
+            m = int(out_c.node_count)
+            n = int(out_c.triangle_count)
+            geometry = CompiledGeometry(
+                triangle_count=n, triangles=out["triangles"], normals=out["normals"], uvs=out["uvs"],
+                tangents=out["tangents"], colors=np.zeros(0, np.float32), materials=out["materials"],
+                flags=out["flags"], sides=out["sides"],
+                bvh=CompiledBvh(out["bounds"][: 6 * m].copy(), out["nodes"][: 3 * m].copy(), m),
+                epsilon=float(out_c.epsilon), order=out["order"][:n].copy())
+        return d, geometry
+
+    def _instance_triangles(self, instances: Sequence[Any]) -> int:
+        if not hasattr(self, "_mesh_tris"):
+            raise RuntimeError("upload_meshes first")
+        return int(sum(self._mesh_tris[int(inst[1])] for inst in instances))
+
+    def send_shading_only(self, scene: CompiledScene) -> int:
+        """Sends a scene's textures and shading (materials, lights, ...) without geometry;
+        returns the shading version, for geometry made by compile_instances."""
+        self._versions += 1
+        sv = self._versions
+        ids = [sv * 100000 + i for i in range(len(scene.textures))]
+        self.send({"type": "textures", "items": [{"id": i, "data": t.data} for i, t in zip(ids, scene.textures)]})
+        self.send({"type": "shading", "version": sv, "shading": ShadingPayload.of(scene, ids)})
+        return sv
 
     # -------------------------------------------------------------- tuning
     def set_timing(self, enabled: bool) -> None:

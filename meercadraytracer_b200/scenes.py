@@ -300,3 +300,104 @@ def orbit_camera(radius: float, height: float, angle_deg: float, target: Tuple[f
     camera.look_at(*target)
     camera.update_matrix_world()
     return camera
+
+
+# ------------------------------------------------------ large instanced scene
+@dataclass
+class InstancedScene:
+    """Instances of one mesh for the per-frame rebuild workload: the mesh, the
+    shading (materials, textures, lights as a CompiledScene without geometry),
+    one material per instance and the camera."""
+
+    name: str
+    mesh: S.BufferGeometry
+    shading: Any  # CompiledScene with geometry None
+    materials: np.ndarray  # material index of each instance
+    camera: S.Camera
+    width: int
+    height: int
+    options: Dict[str, Any]
+    count: int
+    box: float
+    seed: int
+
+    @property
+    def triangles(self) -> int:
+        return self.count * (len(self.mesh.index) // 3 if self.mesh.index is not None else 0)
+
+    def frame(self, k: int) -> List[Tuple[np.ndarray, int, int, int, int, bool]]:
+        """Frame k's instances: rotations uniform on SO(3) (unit quaternions from normal
+        deviates), translations uniform in the box, all re-drawn per frame."""
+        rng = np.random.default_rng(self.seed * 1000003 + k)
+        q = rng.normal(size=(self.count, 4))
+        q /= np.linalg.norm(q, axis=1, keepdims=True)
+        w, x, y, z = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+        r = np.stack([1 - 2 * (y * y + z * z), 2 * (x * y + z * w), 2 * (x * z - y * w),
+                      2 * (x * y - z * w), 1 - 2 * (x * x + z * z), 2 * (y * z + x * w),
+                      2 * (x * z + y * w), 2 * (y * z - x * w), 1 - 2 * (x * x + y * y)], axis=1)
+        t = rng.uniform(-self.box / 2, self.box / 2, (self.count, 3))
+        out = []
+        for i in range(self.count):
+            m = np.zeros(16)
+            m[0:3], m[4:7], m[8:11] = r[i, 0:3], r[i, 3:6], r[i, 6:9]  # columns
+            m[12:15] = t[i]
+            m[15] = 1.0
+            out.append((m, 0, int(self.materials[i]), 7, 0, False))
+        return out
+
+
+def large_scene(seed: int = SEED_BASE + 4, count: int = 4096, subdivisions: int = 5, radius: float = 3.0,
+                box: float = 200.0, width: int = 2048, height: int = 2048, samples: int = 16) -> InstancedScene:
+    """The per-frame rebuild workload: `count` icospheres subdivided `subdivisions` times
+    (20,480 triangles each at 5) under random rigid transforms in a box^3 region, with the
+    mid scene's mix of Standard / transmissive Physical / Phong materials (half with noise
+    albedo maps); 2048 x 2048, 16 spp, GI on, 8 bounces, ACES, sRGB."""
+    from .compile import compile_shading
+
+    rng = np.random.default_rng(seed)
+    v, f = icosphere(subdivisions)
+    p = (v * radius).astype(np.float32)
+    uv = np.stack([np.arctan2(v[:, 2], v[:, 0]) / (2 * math.pi) + 0.5,
+                   np.arcsin(np.clip(v[:, 1], -1, 1)) / math.pi + 0.5], axis=1).astype(np.float32)
+    mesh = S.BufferGeometry(p, v.astype(np.float32), uv, index=f.reshape(-1).astype(np.uint32))
+    # 16 materials drawn like the mid scene's; each instance takes one.
+    shade_scene = S.Scene()
+    for k in range(16):
+        kind = rng.uniform()
+        if kind < 0.4:
+            material: S.Material = S.MeshStandardMaterial(roughness=float(rng.uniform(0, 1)),
+                                                          metalness=float(rng.uniform(0, 1)))
+        elif kind < 0.7:
+            material = S.MeshPhysicalMaterial(transmission=1.0, ior=1.5, roughness=float(rng.uniform(0, 0.2)))
+        else:
+            material = S.MeshPhongMaterial(shininess=float(rng.uniform(1, 200)))
+        material.color = _srgb_color(rng.uniform(0.2, 1.0, 3))
+        if rng.uniform() < 0.5:
+            tex = S.DataTexture(noise_texture(256, seed + 1000 + k), 256, 256)
+            tex.color_space = S.SRGBColorSpace
+            tex.wrap_s = tex.wrap_t = S.RepeatWrapping
+            material.map = tex
+        holder = S.Mesh(S.BufferGeometry(np.zeros((3, 3), np.float32)), material)
+        shade_scene.add(holder)
+    half = box / 2
+    for sx, sz in ((-1, -1), (-1, 1), (1, -1), (1, 1)):
+        light = S.PointLight(0xffffff, 2500.0 * (box / 80.0) ** 2, 0, 2)
+        light.position.set(sx * half * 0.5, half * 1.2, sz * half * 0.5)
+        shade_scene.add(light)
+    shade_scene.add(S.HemisphereLight(0xddeeff, 0x202020, 0.5))
+    shading, _ = compile_shading(shade_scene)
+    from .types import CompiledScene
+
+    compiled = CompiledScene(None, shading.materials, shading.textures, shading.environments,  # type: ignore[arg-type]
+                             shading.lights, shading.background, shading.environment, shading.fog)
+    materials = rng.integers(0, len(shading.materials), count)
+    camera = S.PerspectiveCamera(50, width / height, 0.1, 4000)
+    camera.position.set(0, box * 0.35, box * 1.6)
+    camera.look_at(0, 0, 0)
+    camera.update_matrix_world()
+    tris = count * f.shape[0]
+    return InstancedScene(f"large: {count} icospheres x {f.shape[0]:,} tris = {tris:,} tris, rigid transforms "
+                          f"re-drawn per frame in a {box:g}^3 box, {width}x{height}, {samples} spp, GI on, 8 bounces",
+                          mesh, compiled, materials, camera, width, height,
+                          {"samples": samples, "global_illumination": True, "max_bounces": 8,
+                           "tone_mapping": S.ACESFilmicToneMapping, "output_color_space": "srgb"}, count, box, seed)

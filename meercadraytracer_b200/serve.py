@@ -78,6 +78,7 @@ class RenderServer:
         ex = GpuExecutor(self.device)
         versions = ex.load_scene(scene)
         self.scenes[name] = (ex, versions, scene)
+        self.batch.adopt(scene, ex)
 
     def request(self, client: int, scene: str, camera: CompiledCamera, width: int, height: int,
                 settings: TraceSettings, samples: int = 64, preview_block: int = 8, srgb: bool = True,

@@ -55,7 +55,8 @@ STRUCTS = {
     "mcrt_geometry": abi.mcrt_geometry, "mcrt_shading": abi.mcrt_shading, "mcrt_camera": abi.mcrt_camera,
     "mcrt_settings": abi.mcrt_settings, "mcrt_tile": abi.mcrt_tile, "mcrt_stats": mcrt_stats,
     "mcrt_request": abi.mcrt_request, "mcrt_batch_event": abi.mcrt_batch_event,
-    "mcrt_batch_stats": abi.mcrt_batch_stats,
+    "mcrt_batch_stats": abi.mcrt_batch_stats, "mcrt_mesh": abi.mcrt_mesh, "mcrt_instance": abi.mcrt_instance,
+    "mcrt_build_info": abi.mcrt_build_info, "mcrt_compiled_out": abi.mcrt_compiled_out,
 }
 
 
