@@ -434,52 +434,62 @@ def run_batched(compiled: Dict[str, Any], device: int, capacity: int, seed: int 
         from meercadraytracer_b200 import autotune
 
         choice = autotune.tune_batch(renderer, reqs[:8])
-        # Plain: one raytraceCompiled per request, on executors that already hold the scenes.
-        plain_imgs = []
         execs = {id(c): renderer.executor(c) for c in compiled.values()}
         for ex in execs.values():
-            ex.reset_stats()
             ex.set_capacity(capacity)
             ex.set_traversal(choice.block, choice.stack)
         for r in reqs[:2]:  # warm-up
             execs[id(r.scene)].raytrace(r.scene, r.camera, r.width, r.height, r.settings, 1, True)
-        for ex in execs.values():
-            ex.reset_stats()
-        t0 = time.perf_counter()
-        for r in reqs:
-            plain_imgs.append(execs[id(r.scene)].raytrace(r.scene, r.camera, r.width, r.height, r.settings,
-                                                           r.samples, True))
-        plain_wall = time.perf_counter() - t0
-        pst = [ex.stats() for ex in execs.values()]
-        plain_rays = sum(x["closest_rays"] + x["any_rays"] for x in pst)
-        plain_ms = sum(x["ms_total"] for x in pst)
-        # Batched: the same requests in one batch.
         renderer.render(reqs[:2])  # warm-up (graph instantiation)
-        st0 = renderer.stats()
-        t0 = time.perf_counter()
-        imgs = renderer.render(reqs)
-        batch_wall = time.perf_counter() - t0
-        st1 = renderer.stats()
-        rays = (st1["closest_rays"] - st0["closest_rays"]) + (st1["any_rays"] - st0["any_rays"])
-        gpu_ms = st1["gpu_ms"] - st0["gpu_ms"]
-        same = sum(int(np.array_equal(a, b)) for a, b in zip(imgs, plain_imgs))
-        return {
-            "workload": "64 requests, mid (1,310,720 tris) / small (22,530 tris) scenes 50/50, cameras on a sphere "
-                        "of radius U(10,30) aimed at the origin, resolutions {256^2, 512^2, 640x480, 1024^2}, "
-                        "spp {4, 16, 64}, GI on, 4 bounces; images read back to the host",
-            "requests": len(reqs), "samples": int(sum(r.width * r.height * r.samples for r in reqs)),
-            "rays": int(rays), "plain_rays": int(plain_rays),
-            "plain_mrays_s": round(plain_rays / plain_wall / 1e6, 1),
-            "plain_device_mrays_s": round(plain_rays / (plain_ms / 1e3) / 1e6, 1),
-            "batched_mrays_s": round(rays / batch_wall / 1e6, 1),
-            "batched_device_mrays_s": round(rays / (gpu_ms / 1e3) / 1e6, 1),
-            "speedup_vs_plain": round((rays / batch_wall) / (plain_rays / plain_wall), 3),
-            "plain_wall_s": round(plain_wall, 3), "batched_wall_s": round(batch_wall, 3),
-            "chunks": int(st1["chunks"] - st0["chunks"]), "graph_launches": int(st1["graph_launches"] - st0["graph_launches"]),
-            "capacity": capacity, "images_equal_to_plain": f"{same}/{len(reqs)}",
-            "autotuned": {"block": choice.block, "stack": choice.stack, "chunk": choice.chunk,
-                          "timings_ms": choice.timings},
-        }
+
+        def compare(subset: List[Any]) -> Dict[str, Any]:
+            # Plain: one raytraceCompiled per request, on executors that already hold the scenes.
+            for ex in execs.values():
+                ex.reset_stats()
+            plain_imgs = []
+            t0 = time.perf_counter()
+            for r in subset:
+                plain_imgs.append(execs[id(r.scene)].raytrace(r.scene, r.camera, r.width, r.height, r.settings,
+                                                               r.samples, True))
+            plain_wall = time.perf_counter() - t0
+            pst = [ex.stats() for ex in execs.values()]
+            plain_rays = sum(x["closest_rays"] + x["any_rays"] for x in pst)
+            plain_ms = sum(x["ms_total"] for x in pst)
+            # Batched: the same requests in one batch.
+            st0 = renderer.stats()
+            t0 = time.perf_counter()
+            imgs = renderer.render(subset)
+            batch_wall = time.perf_counter() - t0
+            st1 = renderer.stats()
+            rays = (st1["closest_rays"] - st0["closest_rays"]) + (st1["any_rays"] - st0["any_rays"])
+            gpu_ms = st1["gpu_ms"] - st0["gpu_ms"]
+            same = sum(int(np.array_equal(a, b)) for a, b in zip(imgs, plain_imgs))
+            return {
+                "requests": len(subset), "samples": int(sum(r.width * r.height * r.samples for r in subset)),
+                "rays": int(rays), "plain_rays": int(plain_rays),
+                "plain_mrays_s": round(plain_rays / plain_wall / 1e6, 1),
+                "plain_device_mrays_s": round(plain_rays / (plain_ms / 1e3) / 1e6, 1),
+                "batched_mrays_s": round(rays / batch_wall / 1e6, 1),
+                "batched_device_mrays_s": round(rays / (gpu_ms / 1e3) / 1e6, 1),
+                "speedup_vs_plain": round((rays / batch_wall) / (plain_rays / plain_wall), 3),
+                "plain_wall_s": round(plain_wall, 4), "batched_wall_s": round(batch_wall, 4),
+                "chunks": int(st1["chunks"] - st0["chunks"]),
+                "graph_launches": int(st1["graph_launches"] - st0["graph_launches"]),
+                "images_equal_to_plain": f"{same}/{len(subset)}",
+            }
+
+        out = compare(reqs)
+        out["workload"] = ("64 requests, mid (1,310,720 tris) / small (22,530 tris) scenes 50/50, cameras on a "
+                           "sphere of radius U(10,30) aimed at the origin, resolutions {256^2, 512^2, 640x480, "
+                           "1024^2}, spp {4, 16, 64}, GI on, 4 bounces; images read back to the host")
+        out["capacity"] = capacity
+        out["autotuned"] = {"block": choice.block, "stack": choice.stack, "chunk": choice.chunk,
+                            "timings_ms": choice.timings}
+        # The requests of at most 512^2 pixels and 16 spp: each alone leaves most of the GPU idle.
+        small = [r for r in reqs if r.width * r.height <= 512 * 512 and r.samples <= 16]
+        if small:
+            out["small_requests"] = compare(small)
+        return out
     finally:
         renderer.dispose()
 
