@@ -195,6 +195,22 @@ def run_reference(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def combine_over_ranks(device_ms: float, rays: float, dist: Any, device: str) -> Tuple[float, float]:
+    """Whole-job figures of a replicated run: the slowest rank's device time and every
+    rank's rays (each rank renders its own frame; there is no data exchange). Without a
+    process group, this rank's own figures."""
+    if dist is None:
+        return float(device_ms), float(rays)
+    import torch
+
+    t = torch.tensor([float(device_ms), float(rays)], dtype=torch.float64, device=device)
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    tsum = t.clone()
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return float(tmax[0]), float(tsum[1])
+
+
 def run_ours(args, rank: int, world: int, local: int) -> None:
     import ctypes as C
 
@@ -273,15 +289,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     s = ex.stats()
     device_ms = s["ms_total"]
     rays = s["closest_rays"] + s["any_rays"]
-    t = torch.tensor([device_ms, float(rays)], dtype=torch.float64, device=f"cuda:{local}")
-    if dist:
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t.clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        device_ms, all_rays = float(tmax[0]), float(tsum[1])
-    else:
-        all_rays = float(rays)
+    device_ms, all_rays = combine_over_ranks(device_ms, rays, dist, f"cuda:{local}")
     value = all_rays / (device_ms / 1000.0) / 1e6
     launches = int(s["launches"])
 
