@@ -510,7 +510,7 @@ def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: 
     client's last request runs to 64 spp."""
     from meercadraytracer_b200 import scene as S
     from meercadraytracer_b200.raytrace import trace_settings
-    from meercadraytracer_b200.serve import Client, RenderServer, simulate_clients
+    from meercadraytracer_b200.serve import Client, RenderServer, simulate_clients, simulate_clients_plain
 
     settings = trace_settings({"global_illumination": True, "max_bounces": 4, "tone_mapping": S.ACESFilmicToneMapping})
     orbits = {"small": (17.0, 6.0), "mid": (70.0, 32.0), "big": (130.0, 60.0), "soup": (34.0, 12.0)}
@@ -536,6 +536,9 @@ def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: 
         simulate_clients(server, clients[: len(names)], {n: settings for n in names}, duration=0.2, width=320,
                          height=180, samples=2, seed=1)
         out = simulate_clients(server, clients, {n: settings for n in names}, duration=seconds)
+        # The same clients and moves served by the plain path, one request at a time.
+        out["plain_one_at_a_time"] = simulate_clients_plain(server, clients, {n: settings for n in names},
+                                                            duration=seconds)
         out["scenes"] = {n: int(compiled[n].geometry.triangle_count) for n in names}
         out["capacity"], out["chunk_paths"] = capacity, chunk
         return out

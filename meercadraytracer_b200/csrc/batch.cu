@@ -105,7 +105,7 @@ cudaError_t BatchEngine::init(int device, int capacity, size_t arena_bytes, bool
   if (e == cudaSuccess) e = cudaMemset(counters_dev_, 0, sizeof(BatchCounters));
   if (e == cudaSuccess) e = cudaMemset(tables_dev_, 0, sizeof(BatchTables));
   if (e == cudaSuccess) e = paths_.reserve(capacity_, slots_);
-  if (e == cudaSuccess) e = batch_grids(&grids_);
+  if (e == cudaSuccess) e = batch_grids(&grids_, 0, capacity_);
   return e;
 }
 
@@ -142,7 +142,7 @@ cudaError_t BatchEngine::set_variant(int variant) {
   if (variant == grids_.variant) return cudaSuccess;
   cudaSetDevice(device_);
   cudaError_t e = cudaStreamSynchronize(stream_);
-  if (e == cudaSuccess) e = batch_grids(&grids_, variant);
+  if (e == cudaSuccess) e = batch_grids(&grids_, variant, capacity_);
   graph_valid_ = false;
   return e;
 }

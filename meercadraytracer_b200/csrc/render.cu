@@ -665,6 +665,7 @@ MCRT_D void shade_path(const DScene& sc, const FrameParams& fp, const PathState&
 // still holds the whole shading step without spills, one block more than the
 // compiler's unconstrained choice of 116 registers allows.
 constexpr int kShadeBlocksPerSM = 5;
+constexpr long long kShadeGridFactor = 16;  // batched shading grid, in resident grids
 
 __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSM) k_shade(DScene sc, FrameParams fp, PathState ps,
                                                   const int* __restrict__ qin, int n, int* __restrict__ qout,
@@ -1321,12 +1322,17 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSM) k_batch_shade(DScen
   // reconverges after each path: shading diverges by material, and a warp
   // whose lanes drifted apart across iterations ran each path's code once per
   // lane group (a third of the lanes active, instruction-cache misses).
+  const FrameParams* __restrict__ params = t->fp;
   const int stride = gridDim.x * blockDim.x;
+#pragma unroll 1
   for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
     const int q = base + threadIdx.x;
     if (q < n) {
       const int pid = qin[q];
-      shade_path(sc, t->fp[ps.seg[pid]], ps, pid, qs);
+      // The segment's parameters through a read-only, non-aliasing view of
+      // the table: through `t` itself every field would be reloaded after
+      // each store of the shading step, one dependent L1 round trip each.
+      shade_path(sc, params[ps.seg[pid]], ps, pid, qs);
     }
     __syncwarp();
   }
@@ -1356,12 +1362,13 @@ __global__ void __launch_bounds__(kBlock) k_batch_resolve(DScene sc, int s, Batc
   SceneQueues* sq = &t->scenes[s];
   const int n = static_cast<int>(sq->count);
   const int* qin = ps.queue[t->iteration & 1] + sq->base;
+  const FrameParams* __restrict__ params = t->fp;
   const int stride = gridDim.x * blockDim.x;
   for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
     const int q = base + threadIdx.x;
     if (q < n) {
       const int pid = qin[q];
-      resolve_path(sc, t->fp[ps.seg[pid]], ps, pid, capacity);
+      resolve_path(sc, params[ps.seg[pid]], ps, pid, capacity);
     }
     __syncwarp();
   }
@@ -1466,13 +1473,21 @@ const BatchVariant& batch_variant(int v) { return kBatchVariants[(v >= 0 && v < 
 
 }  // namespace
 
-cudaError_t batch_grids(BatchGrids* g, int variant) {
+cudaError_t batch_grids(BatchGrids* g, int variant, int capacity) {
   const BatchVariant& bv = batch_variant(variant);
   g->variant = (variant >= 0 && variant < kVariantCount) ? variant : 0;
   g->block = bv.block;
   g->raygen = resident_blocks(reinterpret_cast<const void*>(k_batch_raygen), kBlock);
   g->extend = resident_blocks(reinterpret_cast<const void*>(bv.extend), bv.block);
-  g->shade = resident_blocks(reinterpret_cast<const void*>(k_batch_shade), kBlock);
+  // Shading launches many more blocks than fit at once (each taking a few
+  // 128-path tiles): blocks that finish make room for fresh ones, as in the
+  // one-path-per-thread launch of the plain path, instead of a resident grid
+  // whose warps stay in the shading code for every tile.
+  {
+    const int resident = resident_blocks(reinterpret_cast<const void*>(k_batch_shade), kBlock);
+    const long long tiles = (static_cast<long long>(std::max(capacity, 1)) + kBlock - 1) / kBlock;
+    g->shade = static_cast<int>(std::max<long long>(resident, std::min<long long>(tiles, kShadeGridFactor * resident)));
+  }
   g->shadow = resident_blocks(reinterpret_cast<const void*>(bv.shadow), bv.block);
   g->resolve = resident_blocks(reinterpret_cast<const void*>(k_batch_resolve), kBlock);
   g->accumulate = resident_blocks(reinterpret_cast<const void*>(k_batch_accumulate), 256);

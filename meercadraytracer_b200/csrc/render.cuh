@@ -181,7 +181,7 @@ struct BatchGrids {
   int variant, block;
 };
 
-cudaError_t batch_grids(BatchGrids* g, int variant = 0);
+cudaError_t batch_grids(BatchGrids* g, int variant, int capacity);
 
 // Traversal variants: the closest-hit and shadow kernels compiled for several
 // (threads per block, shared-memory short-stack entries per thread) pairs.

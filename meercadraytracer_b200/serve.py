@@ -253,3 +253,70 @@ def simulate_clients(server: RenderServer, clients: Sequence[Client], settings: 
         settled = [(r.done - r.arrival) * 1e3 for r in last.values() if r.done is not None]
         out["settled_time_to_done_ms"] = {"p50": _pct(settled, 50), "p99": _pct(settled, 99), "count": len(settled)}
     return out
+
+
+def simulate_clients_plain(server: RenderServer, clients: Sequence[Client], settings: Dict[str, TraceSettings],
+                           duration: float = 10.0, mean_interval: float = 0.1, width: int = 1280, height: int = 720,
+                           samples: int = 64, preview_block: int = 8, seed: int = 0x5EED0003) -> Dict[str, Any]:
+    """The same clients and camera moves served by the plain path, one request at a time:
+    each client's latest request, oldest first, gets its block preview (one tile render
+    with block `preview_block`, as the reference's ProgressiveRenderer starts) and then,
+    unless the client has moved on meanwhile, its full render (one raytraceCompiled call of
+    `samples` passes, which cannot be interrupted). Uses the server's resident scenes; no
+    batching, no overlap. Returns the same figures as simulate_clients (without settling)."""
+    from .compile import compile_camera
+    from .scenes import orbit_camera
+    from .types import Tile
+
+    moves = arrival_times(len(clients), duration, mean_interval, seed)
+    execs = {name: (ex, versions, scene) for name, (ex, versions, scene) in server.scenes.items()}
+    for ex, _, _ in execs.values():
+        ex.reset_stats()
+    clock = server.clock
+    t0 = clock()
+    latest: Dict[int, Tuple[float, int]] = {}  # client -> (arrival, move index)
+    served: List[Dict[str, Any]] = []
+    i = 0
+    requests = 0
+    while True:
+        now = clock() - t0
+        while i < len(moves) and moves[i][0] <= now:
+            latest[moves[i][1]] = (moves[i][0], i)
+            requests += 1
+            i += 1
+        if now >= duration:
+            break
+        if not latest:
+            time.sleep(max(0.0, min(0.002, moves[i][0] - now)) if i < len(moves) else 0.002)
+            continue
+        c, (t_arr, k) = min(latest.items(), key=lambda kv: kv[1][0])
+        del latest[c]
+        cl = clients[c]
+        ex, (gv, sv), scene = execs[cl.scene]
+        cam = compile_camera(orbit_camera(cl.radius, cl.height, cl.phase + cl.speed * t_arr, cl.target,
+                                          aspect=width / height))
+        rec: Dict[str, Any] = {"arrival": t0 + t_arr, "preview": None, "done": None}
+        if preview_block > 1:
+            ex.render({"type": "tile", "job": k, "geometry_version": gv, "shading_version": sv, "camera": cam,
+                       "settings": settings[cl.scene], "tile": Tile(0, 0, width, height), "width": width,
+                       "height": height, "pass": 0, "block": preview_block}).result()
+            rec["preview"] = clock()
+        # A newer move of this client (arrived while previewing) restarts it: no full render.
+        now = clock() - t0
+        while i < len(moves) and moves[i][0] <= now:
+            latest[moves[i][1]] = (moves[i][0], i)
+            requests += 1
+            i += 1
+        if c not in latest:
+            ex.raytrace(scene, cam, width, height, settings[cl.scene], samples, True)
+            rec["done"] = clock()
+        served.append(rec)
+    t_end = clock() - t0
+    rays = sum(e.stats()["closest_rays"] + e.stats()["any_rays"] for e, _, _ in execs.values())
+    ttp = [(r["preview"] - r["arrival"]) * 1e3 for r in served if r["preview"] is not None]
+    ttd = [(r["done"] - r["arrival"]) * 1e3 for r in served if r["done"] is not None]
+    return {"clients": len(clients), "wall_s": round(t_end, 3), "requests": requests, "previews": len(ttp),
+            "completed": len(ttd),
+            "time_to_preview_ms": {"p50": _pct(ttp, 50), "p99": _pct(ttp, 99), "max": max(ttp) if ttp else None},
+            "time_to_64spp_ms": {"p50": _pct(ttd, 50), "p99": _pct(ttd, 99), "count": len(ttd)},
+            "mrays_s": rays / t_end / 1e6 if t_end > 0 else 0.0, "rays": int(rays)}

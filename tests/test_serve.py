@@ -59,3 +59,21 @@ def test_served_requests_equal_plain_renders():
         assert st["arena_used"] == 0 and st["status"] == 0
     finally:
         server.close()
+
+
+@pytest.mark.gpu
+def test_plain_one_at_a_time_serving_runs_the_same_clients():
+    from meercadraytracer_b200.serve import simulate_clients_plain
+
+    small = scenes.small_scene()
+    compiled = compile_scene(small.scene, builder=cpu.compile_sink)
+    gi = trace_settings(as_options({"global_illumination": True, "max_bounces": 4}))
+    server = RenderServer(capacity=1 << 15, memory_budget=8 << 20)
+    try:
+        server.add_scene("small", compiled)
+        clients = [Client("small", 17.0, 6.0), Client("small", 20.0, 4.0, phase=90)]
+        out = simulate_clients_plain(server, clients, {"small": gi}, duration=0.5, width=64, height=36, samples=4)
+        assert out["requests"] >= 2 and out["previews"] >= 1
+        assert out["time_to_preview_ms"]["p50"] is not None and out["rays"] > 0
+    finally:
+        server.close()
