@@ -472,6 +472,8 @@ def run_batched(compiled: Dict[str, Any], device: int, capacity: int, seed: int 
             rays = (st1["closest_rays"] - st0["closest_rays"]) + (st1["any_rays"] - st0["any_rays"])
             gpu_ms = st1["gpu_ms"] - st0["gpu_ms"]
             same = sum(int(np.array_equal(a, b)) for a, b in zip(imgs, plain_imgs))
+            near = sum(int(np.abs(a.astype(np.int16) - b.astype(np.int16)).max(initial=0) <= 1)
+                       for a, b in zip(imgs, plain_imgs))
             return {
                 "requests": len(subset), "samples": int(sum(r.width * r.height * r.samples for r in subset)),
                 "rays": int(rays), "plain_rays": int(plain_rays),
@@ -484,6 +486,7 @@ def run_batched(compiled: Dict[str, Any], device: int, capacity: int, seed: int 
                 "chunks": int(st1["chunks"] - st0["chunks"]),
                 "graph_launches": int(st1["graph_launches"] - st0["graph_launches"]),
                 "images_equal_to_plain": f"{same}/{len(subset)}",
+                "images_within_one_level_of_plain": f"{near}/{len(subset)}",
             }
 
         out = compare(reqs)

@@ -34,6 +34,7 @@ namespace mcrt {
 
 constexpr int kBlock = 128;
 constexpr int kShadowSeen = 16;  // de-duplicated see-through hits per shadow ray
+constexpr int kSortMin = 1 << 16;  // shorter queues are shaded in the order they are in
 constexpr int kMaxIterations = 1 << 16;  // bounce / pass-through iterations of one chunk
 
 // Appends to a queue counter with one atomic per coalesced group of threads.
@@ -146,10 +147,10 @@ struct ExtendQuery {
 };
 
 // B threads per block, S short-stack entries per thread (a traversal variant).
-// 1024 / B blocks per SM: the register cap (64) costs a few bytes of spills
-// and buys an eighth more resident warps than the unconstrained 72 registers.
+// 1280 / B blocks per SM: the register cap (48) costs a few bytes of spills
+// and buys a ninth more resident warps than the unconstrained 56 registers.
 template <int B, int S>
-__global__ void __launch_bounds__(B) k_extend(DScene sc, PathState ps, const int* __restrict__ queue, int n,
+__global__ void __launch_bounds__(B, 1280 / B) k_extend(DScene sc, PathState ps, const int* __restrict__ queue, int n,
                                               Counters* cnt) {
   __shared__ int stack_mem[S * B];
   TravStackT<S> st;
@@ -160,6 +161,56 @@ __global__ void __launch_bounds__(B) k_extend(DScene sc, PathState ps, const int
   ExtendQuery q{sc, ps, queue, 0, {}};
   traverse_persistent(sc, q, n, &cnt->fetch, st, status);
   if (status) atomicOr(&cnt->status, status);
+}
+
+// ------------------------------------------------------- shading order
+// The shading step branches on what a path hit: nothing (background), or a
+// material of one model, transmissive or not. Shading the queue in that
+// class order gives each warp lanes that take the same branches (and run
+// the same code) instead of a mix; results do not depend on queue order.
+constexpr int kShadeClasses = 16;
+
+MCRT_D int shade_class(const DScene& sc, const PathState& ps, int pid) {
+  const unsigned word = __float_as_uint(ps.hit[pid].w);
+  const int tri = static_cast<int>(word & 0x7fffffffu) - 1;
+  if (tri < 0) return 0;
+  const int m = __float_as_int(__ldg(&sc.tris[3 * static_cast<size_t>(tri) + 1].w));
+  const DMaterial& mat = sc.materials[m];
+  return 1 + 2 * min(max(mat.model, 0), 6) + (mat.transmission > 0.0f ? 1 : 0);
+}
+
+__global__ void __launch_bounds__(256) k_class_count(DScene sc, PathState ps, const int* __restrict__ queue, int n,
+                                                     unsigned int* __restrict__ bins) {
+  __shared__ unsigned int h[kShadeClasses];
+  if (threadIdx.x < kShadeClasses) h[threadIdx.x] = 0;
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(&h[shade_class(sc, ps, queue[i])], 1u);
+  __syncthreads();
+  if (threadIdx.x < kShadeClasses && h[threadIdx.x]) atomicAdd(&bins[threadIdx.x], h[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(256) k_class_scatter(DScene sc, PathState ps, const int* __restrict__ queue, int n,
+                                                       unsigned int* __restrict__ bins, int* __restrict__ out) {
+  __shared__ unsigned int base[kShadeClasses];
+  if (threadIdx.x == 0) {
+    unsigned int sum = 0;
+    for (int b = 0; b < kShadeClasses; b++) {
+      base[b] = sum;
+      sum += bins[b];
+    }
+  }
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int pid = queue[i];
+  const int c = shade_class(sc, ps, pid);
+  const unsigned int peers = __match_any_sync(__activemask(), c);
+  const int leader = __ffs(peers) - 1;
+  unsigned int b = 0;
+  if (static_cast<int>(threadIdx.x & 31) == leader) b = atomicAdd(&bins[kShadeClasses + c], __popc(peers));
+  b = __shfl_sync(peers, b, leader);
+  out[base[c] + b + __popc(peers & lanemask_lt())] = pid;
 }
 
 // ------------------------------------------------------------------- shade
@@ -1031,6 +1082,17 @@ cudaError_t PathBuffers::reserve(int capacity, int slots) {
     e = alloc(sizeof(int) * n, &p);
     st_.queue[i] = static_cast<int*>(p);
   }
+  if (e == cudaSuccess) {
+    void* p = nullptr;
+    e = alloc(sizeof(int) * n, &p);
+    st_.binned = static_cast<int*>(p);
+  }
+  if (e == cudaSuccess) {
+    void* p = nullptr;
+    e = alloc(sizeof(unsigned int) * 2 * kShadeClasses * kMaxBatchScenes, &p);
+    st_.bins = static_cast<unsigned int*>(p);
+    if (e == cudaSuccess) e = cudaMemset(p, 0, sizeof(unsigned int) * 2 * kShadeClasses * kMaxBatchScenes);
+  }
   if (e == cudaSuccess) e = cudaMalloc(&counters_, sizeof(Counters));
   if (e == cudaSuccess) e = cudaMallocHost(&host_counters_, sizeof(Counters));
   if (e != cudaSuccess) {
@@ -1179,8 +1241,16 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
       tm.stop(st.ms_extend, st.n_extend);
       st.closest_rays += n;
       cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), stream);
+      const int* shade_queue = ps.queue[cur];
+      if (sort_shading && n >= kSortMin) {
+        cudaMemsetAsync(ps.bins, 0, 2 * kShadeClasses * sizeof(unsigned int), stream);
+        k_class_count<<<blocks_for(n, 256), 256, 0, stream>>>(scene, ps, ps.queue[cur], n, ps.bins);
+        k_class_scatter<<<blocks_for(n, 256), 256, 0, stream>>>(scene, ps, ps.queue[cur], n, ps.bins, ps.binned);
+        shade_queue = ps.binned;
+        st.launches += 2;
+      }
       tm.start();
-      k_shade<<<blocks_for(n, kBlock), kBlock, 0, stream>>>(scene, f, ps, ps.queue[cur], n, ps.queue[cur ^ 1], cnt);
+      k_shade<<<blocks_for(n, kBlock), kBlock, 0, stream>>>(scene, f, ps, shade_queue, n, ps.queue[cur ^ 1], cnt);
       tm.stop(st.ms_shade, st.n_shade);
       cudaMemcpyAsync(host, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, stream);
       e = cudaStreamSynchronize(stream);
@@ -1315,7 +1385,8 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSM) k_batch_shade(DScen
   SceneQueues* sq = &t->scenes[s];
   const int n = static_cast<int>(sq->count);
   const int cur = t->iteration & 1;
-  const int* qin = ps.queue[cur] + sq->base;
+  // In shading order once the queue is long enough to be sorted (k_batch_class_*).
+  const int* qin = (n >= kSortMin ? ps.binned : ps.queue[cur]) + sq->base;
   const StageQueues qs{ps.queue[cur ^ 1] + sq->base, &sq->next_count,
                        ps.shadow_queue + 3ull * sq->base * static_cast<unsigned>(slots), &sq->shadow_count};
   // Every lane of a warp runs the same number of iterations and the warp
@@ -1374,10 +1445,60 @@ __global__ void __launch_bounds__(kBlock) k_batch_resolve(DScene sc, int s, Batc
   }
 }
 
+// Shading order of one scene's queue range (k_class_count / k_class_scatter
+// over a resident grid): bins of scene s are bins[32 s, 32 s + 32).
+__global__ void __launch_bounds__(256) k_batch_class_count(DScene sc, int s, BatchTables* t, PathState ps) {
+  SceneQueues* sq = &t->scenes[s];
+  const int n = static_cast<int>(sq->count);
+  if (n < kSortMin) return;
+  const int* qin = ps.queue[t->iteration & 1] + sq->base;
+  unsigned int* bins = ps.bins + 2 * kShadeClasses * s;
+  __shared__ unsigned int h[kShadeClasses];
+  if (threadIdx.x < kShadeClasses) h[threadIdx.x] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    atomicAdd(&h[shade_class(sc, ps, qin[i])], 1u);
+  __syncthreads();
+  if (threadIdx.x < kShadeClasses && h[threadIdx.x]) atomicAdd(&bins[threadIdx.x], h[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(256) k_batch_class_scatter(DScene sc, int s, BatchTables* t, PathState ps) {
+  SceneQueues* sq = &t->scenes[s];
+  const int n = static_cast<int>(sq->count);
+  if (n < kSortMin) return;
+  const int* qin = ps.queue[t->iteration & 1] + sq->base;
+  unsigned int* bins = ps.bins + 2 * kShadeClasses * s;
+  int* out = ps.binned + sq->base;
+  __shared__ unsigned int base[kShadeClasses];
+  if (threadIdx.x == 0) {
+    unsigned int sum = 0;
+    for (int b = 0; b < kShadeClasses; b++) {
+      base[b] = sum;
+      sum += bins[b];
+    }
+  }
+  __syncthreads();
+  const int stride = gridDim.x * blockDim.x;
+  for (int first = blockIdx.x * blockDim.x; first < n; first += stride) {
+    const int i = first + threadIdx.x;
+    if (i < n) {
+      const int pid = qin[i];
+      const int c = shade_class(sc, ps, pid);
+      const unsigned int peers = __match_any_sync(__activemask(), c);
+      const int leader = __ffs(peers) - 1;
+      unsigned int b = 0;
+      if (static_cast<int>(threadIdx.x & 31) == leader) b = atomicAdd(&bins[kShadeClasses + c], __popc(peers));
+      b = __shfl_sync(peers, b, leader);
+      out[base[c] + b + __popc(peers & lanemask_lt())] = pid;
+    }
+    __syncwarp();
+  }
+}
+
 // Queue swap after an iteration, on one thread: counts the queries traced,
 // makes the continued paths the next iteration's queue and says whether
 // another iteration is needed.
-__global__ void k_batch_advance(BatchTables* t, int nscenes, BatchCounters* bc, int graph,
+__global__ void k_batch_advance(BatchTables* t, int nscenes, BatchCounters* bc, unsigned int* bins, int graph,
                                 cudaGraphConditionalHandle handle) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   bool more = false;
@@ -1395,6 +1516,7 @@ __global__ void k_batch_advance(BatchTables* t, int nscenes, BatchCounters* bc, 
   }
   bc->closest += closest;
   bc->any += any;
+  for (int i = 0; i < 2 * kShadeClasses * nscenes; i++) bins[i] = 0;  // the next iteration's shading order
   const int it = t->iteration + 1;
   t->iteration = it;
   if (more && it >= t->max_iterations) {
@@ -1491,6 +1613,7 @@ cudaError_t batch_grids(BatchGrids* g, int variant, int capacity) {
   g->shadow = resident_blocks(reinterpret_cast<const void*>(bv.shadow), bv.block);
   g->resolve = resident_blocks(reinterpret_cast<const void*>(k_batch_resolve), kBlock);
   g->accumulate = resident_blocks(reinterpret_cast<const void*>(k_batch_accumulate), 256);
+  g->sort = resident_blocks(reinterpret_cast<const void*>(k_batch_class_scatter), 256);
   return cudaGetLastError();
 }
 
@@ -1504,11 +1627,13 @@ cudaError_t launch_batch_iteration(const DScene* scenes, int nscenes, BatchTable
                                    cudaGraphConditionalHandle handle, cudaStream_t s) {
   const BatchVariant& bv = batch_variant(g.variant);
   for (int i = 0; i < nscenes; i++) bv.extend<<<g.extend, bv.block, 0, s>>>(scenes[i], i, t, ps, counters);
+  for (int i = 0; i < nscenes; i++) k_batch_class_count<<<g.sort, 256, 0, s>>>(scenes[i], i, t, ps);
+  for (int i = 0; i < nscenes; i++) k_batch_class_scatter<<<g.sort, 256, 0, s>>>(scenes[i], i, t, ps);
   for (int i = 0; i < nscenes; i++) k_batch_shade<<<g.shade, kBlock, 0, s>>>(scenes[i], i, t, ps, slots);
   for (int i = 0; i < nscenes; i++)
     bv.shadow<<<g.shadow, bv.block, 0, s>>>(scenes[i], i, t, ps, capacity, slots, counters);
   for (int i = 0; i < nscenes; i++) k_batch_resolve<<<g.resolve, kBlock, 0, s>>>(scenes[i], i, t, ps, capacity);
-  k_batch_advance<<<1, 32, 0, s>>>(t, nscenes, counters, graph ? 1 : 0, handle);
+  k_batch_advance<<<1, 32, 0, s>>>(t, nscenes, counters, ps.bins, graph ? 1 : 0, handle);
   return cudaGetLastError();
 }
 

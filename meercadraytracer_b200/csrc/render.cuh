@@ -59,6 +59,8 @@ struct PathState {
   float4* sample;  // finished sample: premultiplied, tone mapped RGBA
   float4* slots;   // [slot][capacity] shadow contributions
   int* queue[2];
+  int* binned;           // the queue in shading order
+  unsigned int* bins;    // class counts and cursors of that order
   float4* shadow_queue;  // 3 float4 per shadow ray
   int* seg;              // batched renders: the segment each path belongs to
 };
@@ -112,6 +114,7 @@ class PathBuffers {
 class Wavefront {
  public:
   int variant = 0;  // traversal variant (see traversal_variant_info)
+  bool sort_shading = true;  // shade each bounce's paths grouped by what they hit
   cudaError_t run(const DScene& scene, FrameParams fp, int passes, PathBuffers& buffers, cudaStream_t stream,
                   RenderStats* stats, bool timed,
                   cudaError_t (*on_chunk)(void* ctx, int first_pass, int pass_count), void* ctx);
@@ -177,7 +180,7 @@ struct BatchCounters {
 
 // Grid sizes of the batched kernels on the current device, for a traversal variant.
 struct BatchGrids {
-  int raygen, extend, shade, shadow, resolve, accumulate;
+  int raygen, extend, shade, shadow, resolve, accumulate, sort;
   int variant, block;
 };
 
