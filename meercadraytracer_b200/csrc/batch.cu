@@ -78,6 +78,11 @@ BatchEngine::~BatchEngine() {
     if (c.copied) cudaEventDestroy(c.copied);
   }
   if (last_copy_) cudaEventDestroy(last_copy_);
+  for (int i = 0; i < kMaxBatchScenes; i++) {
+    if (lanes_.stream[i]) cudaStreamDestroy(lanes_.stream[i]);
+    if (lanes_.join[i]) cudaEventDestroy(lanes_.join[i]);
+  }
+  if (lanes_.fork) cudaEventDestroy(lanes_.fork);
   destroy_graph();
   if (tables_dev_) cudaFree(tables_dev_);
   for (BatchTables* t : tables_host_)
@@ -96,6 +101,11 @@ cudaError_t BatchEngine::init(int device, int capacity, size_t arena_bytes, bool
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&last_copy_, cudaEventDisableTiming);
+  for (int i = 0; i < kMaxBatchScenes && e == cudaSuccess; i++) {
+    e = cudaStreamCreateWithFlags(&lanes_.stream[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&lanes_.join[i], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&lanes_.fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = arena_.init(arena_bytes);
   if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&tables_dev_), sizeof(BatchTables));
   for (int i = 0; i < 2 && e == cudaSuccess; i++)
@@ -190,7 +200,7 @@ cudaError_t BatchEngine::ensure_graph() {
   e = cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, mode);
   if (e != cudaSuccess) return e;
   le = launch_batch_iteration(scenes_, nscenes_, tables_dev_, ps, paths_.capacity(), paths_.slots(), counters_dev_,
-                              grids_, true, handle, stream_);
+                              grids_, true, handle, stream_, &lanes_);
   e = cudaStreamEndCapture(stream_, &body);
   if (e == cudaSuccess) e = le;
   if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(stream_, graph_, &loop, nullptr, 1, mode);

@@ -149,6 +149,7 @@ class BatchEngine {
   int slots_ = 1;
   bool use_graph_ = true;
   cudaStream_t stream_ = nullptr, copy_stream_ = nullptr;
+  SceneLanes lanes_{};  // per-scene branches of the captured bounce iteration
   PathBuffers paths_;
   DeviceArena arena_;
   BatchTables* tables_dev_ = nullptr;

@@ -1624,15 +1624,34 @@ cudaError_t launch_batch_raygen(const BatchTables* t, const PathState& ps, const
 
 cudaError_t launch_batch_iteration(const DScene* scenes, int nscenes, BatchTables* t, const PathState& ps,
                                    int capacity, int slots, BatchCounters* counters, const BatchGrids& g, bool graph,
-                                   cudaGraphConditionalHandle handle, cudaStream_t s) {
+                                   cudaGraphConditionalHandle handle, cudaStream_t s, const SceneLanes* lanes) {
   const BatchVariant& bv = batch_variant(g.variant);
-  for (int i = 0; i < nscenes; i++) bv.extend<<<g.extend, bv.block, 0, s>>>(scenes[i], i, t, ps, counters);
-  for (int i = 0; i < nscenes; i++) k_batch_class_count<<<g.sort, 256, 0, s>>>(scenes[i], i, t, ps);
-  for (int i = 0; i < nscenes; i++) k_batch_class_scatter<<<g.sort, 256, 0, s>>>(scenes[i], i, t, ps);
-  for (int i = 0; i < nscenes; i++) k_batch_shade<<<g.shade, kBlock, 0, s>>>(scenes[i], i, t, ps, slots);
-  for (int i = 0; i < nscenes; i++)
-    bv.shadow<<<g.shadow, bv.block, 0, s>>>(scenes[i], i, t, ps, capacity, slots, counters);
-  for (int i = 0; i < nscenes; i++) k_batch_resolve<<<g.resolve, kBlock, 0, s>>>(scenes[i], i, t, ps, capacity);
+  // One scene's stages, in order: closest hits, shading order, shading, shadow
+  // rays, resolve. Scenes touch disjoint queue ranges, bins and slots.
+  auto chain = [&](int i, cudaStream_t q) {
+    bv.extend<<<g.extend, bv.block, 0, q>>>(scenes[i], i, t, ps, counters);
+    k_batch_class_count<<<g.sort, 256, 0, q>>>(scenes[i], i, t, ps);
+    k_batch_class_scatter<<<g.sort, 256, 0, q>>>(scenes[i], i, t, ps);
+    k_batch_shade<<<g.shade, kBlock, 0, q>>>(scenes[i], i, t, ps, slots);
+    bv.shadow<<<g.shadow, bv.block, 0, q>>>(scenes[i], i, t, ps, capacity, slots, counters);
+    k_batch_resolve<<<g.resolve, kBlock, 0, q>>>(scenes[i], i, t, ps, capacity);
+  };
+  cudaError_t e = cudaSuccess;
+  if (lanes && nscenes > 1) {
+    // The scenes' chains as parallel branches: one scene's kernels fill the
+    // tails of another's instead of waiting for them.
+    e = cudaEventRecord(lanes->fork, s);
+    for (int i = 0; i < nscenes && e == cudaSuccess; i++) {
+      e = cudaStreamWaitEvent(lanes->stream[i], lanes->fork, 0);
+      if (e != cudaSuccess) break;
+      chain(i, lanes->stream[i]);
+      e = cudaEventRecord(lanes->join[i], lanes->stream[i]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s, lanes->join[i], 0);
+    }
+  } else {
+    for (int i = 0; i < nscenes; i++) chain(i, s);
+  }
+  if (e != cudaSuccess) return e;
   k_batch_advance<<<1, 32, 0, s>>>(t, nscenes, counters, ps.bins, graph ? 1 : 0, handle);
   return cudaGetLastError();
 }

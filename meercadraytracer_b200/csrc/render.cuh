@@ -198,9 +198,18 @@ cudaError_t launch_batch_raygen(const BatchTables* t, const PathState& ps, const
 // rays, resolve, then the queue swap. `graph`: the swap sets conditional
 // `handle` (the loop runs as a graph's while node); otherwise it sets
 // counters->more for a host-driven loop.
+// Streams and events that run each scene's stages as a parallel branch of a
+// captured iteration (fork from the iteration's stream, join before advance).
+struct SceneLanes {
+  cudaStream_t stream[kMaxBatchScenes];
+  cudaEvent_t fork;
+  cudaEvent_t join[kMaxBatchScenes];
+};
+
 cudaError_t launch_batch_iteration(const DScene* scenes, int nscenes, BatchTables* t, const PathState& ps,
                                    int capacity, int slots, BatchCounters* counters, const BatchGrids& g, bool graph,
-                                   cudaGraphConditionalHandle handle, cudaStream_t s);
+                                   cudaGraphConditionalHandle handle, cudaStream_t s,
+                                   const SceneLanes* lanes = nullptr);
 // Accumulates (or, for previews, writes) every segment's samples and encodes
 // the requests' images.
 cudaError_t launch_batch_accumulate(const BatchTables* t, const PathState& ps, const BatchGrids& g, cudaStream_t s);
