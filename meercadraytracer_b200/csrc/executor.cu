@@ -208,6 +208,7 @@ struct mcrt_executor {
   RenderStats stats;
   double ms_total = 0;
   DevBuf sum, image, list_x, list_y, out_tile, rays, hits, scratch;
+  DevBuf pack_flag, pack_index, pack_temp;  // node packing of device-compiled geometry, kept across rebuilds
   DevBuf dfg_buf, srgb_lut;
   cudaTextureObject_t dfg_tex = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1057,17 +1058,24 @@ int32_t mcrt_compile_instances(mcrt_executor* ex, int32_t version, int32_t count
                  "copy");
       k_mark_leaf_ends<<<blocks(m, 256), 256, 0, s>>>(g.nodes, m, G.tris.as<float4>());
       if (G.root_count == 0) {
-        // A full binary tree of m nodes has (m - 1) / 2 inner nodes.
-        DevBuf flag, index, temp;
-        flag.ensure(sizeof(int) * m);
-        index.ensure(sizeof(int) * m);
+        // A full binary tree of m nodes has (m - 1) / 2 inner nodes; buffers
+        // are sized for the most any build of n triangles can make, so a
+        // rebuild every frame allocates (and synchronises) nothing.
+        DevBuf& flag = ex->pack_flag;
+        DevBuf& index = ex->pack_index;
+        DevBuf& temp = ex->pack_temp;
+        const size_t m_cap = 2 * static_cast<size_t>(n);
+        flag.ensure(sizeof(int) * m_cap);
+        index.ensure(sizeof(int) * m_cap);
         k_inner_flags<<<blocks(m, 256), 256, 0, s>>>(g.nodes, m, flag.as<int>());
         size_t temp_bytes = 0;
-        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, flag.as<int>(), index.as<int>(), m, s), "scan");
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, flag.as<int>(), index.as<int>(),
+                                                 static_cast<int>(m_cap), s),
+                   "scan");
         temp.ensure(temp_bytes);
         cuda_check(cub::DeviceScan::ExclusiveSum(temp.as<void>(), temp_bytes, flag.as<int>(), index.as<int>(), m, s),
                    "scan");
-        G.nodes.ensure(sizeof(DNode) * std::max((m - 1) / 2, 1));
+        G.nodes.ensure(sizeof(DNode) * std::max(n - 1, 1));
         k_pack_nodes<<<blocks(m, 256), 256, 0, s>>>(g.bounds, g.nodes, index.as<int>(), m, G.nodes.as<DNode>());
         cuda_check(cudaGetLastError(), "BVH conversion");
         cuda_check(cudaStreamSynchronize(s), "geometry pack");

@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(B, 1280 / B) k_extend(DScene sc, PathState ps,
 constexpr int kShadeClasses = 16;
 
 MCRT_D int shade_class(const DScene& sc, const PathState& ps, int pid) {
-  const unsigned word = __float_as_uint(ps.hit[pid].w);
+  const unsigned word = __float_as_uint(__ldg(reinterpret_cast<const float*>(ps.hit + pid) + 3));
   const int tri = static_cast<int>(word & 0x7fffffffu) - 1;
   if (tri < 0) return 0;
   const int m = __float_as_int(__ldg(&sc.tris[3 * static_cast<size_t>(tri) + 1].w));
@@ -185,7 +185,11 @@ __global__ void __launch_bounds__(256) k_class_count(DScene sc, PathState ps, co
   if (threadIdx.x < kShadeClasses) h[threadIdx.x] = 0;
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) atomicAdd(&h[shade_class(sc, ps, queue[i])], 1u);
+  if (i < n) {
+    const int c = shade_class(sc, ps, queue[i]);
+    ps.cls[i] = static_cast<uint8_t>(c);  // kept for the scatter, by queue position
+    atomicAdd(&h[c], 1u);
+  }
   __syncthreads();
   if (threadIdx.x < kShadeClasses && h[threadIdx.x]) atomicAdd(&bins[threadIdx.x], h[threadIdx.x]);
 }
@@ -204,7 +208,7 @@ __global__ void __launch_bounds__(256) k_class_scatter(DScene sc, PathState ps, 
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int pid = queue[i];
-  const int c = shade_class(sc, ps, pid);
+  const int c = ps.cls[i];
   const unsigned int peers = __match_any_sync(__activemask(), c);
   const int leader = __ffs(peers) - 1;
   unsigned int b = 0;
@@ -1089,6 +1093,11 @@ cudaError_t PathBuffers::reserve(int capacity, int slots) {
   }
   if (e == cudaSuccess) {
     void* p = nullptr;
+    e = alloc(n, &p);
+    st_.cls = static_cast<uint8_t*>(p);
+  }
+  if (e == cudaSuccess) {
+    void* p = nullptr;
     e = alloc(sizeof(unsigned int) * 2 * kShadeClasses * kMaxBatchScenes, &p);
     st_.bins = static_cast<unsigned int*>(p);
     if (e == cudaSuccess) e = cudaMemset(p, 0, sizeof(unsigned int) * 2 * kShadeClasses * kMaxBatchScenes);
@@ -1456,8 +1465,12 @@ __global__ void __launch_bounds__(256) k_batch_class_count(DScene sc, int s, Bat
   __shared__ unsigned int h[kShadeClasses];
   if (threadIdx.x < kShadeClasses) h[threadIdx.x] = 0;
   __syncthreads();
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    atomicAdd(&h[shade_class(sc, ps, qin[i])], 1u);
+  uint8_t* cls = ps.cls + sq->base;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = shade_class(sc, ps, qin[i]);
+    cls[i] = static_cast<uint8_t>(c);
+    atomicAdd(&h[c], 1u);
+  }
   __syncthreads();
   if (threadIdx.x < kShadeClasses && h[threadIdx.x]) atomicAdd(&bins[threadIdx.x], h[threadIdx.x]);
 }
@@ -1483,7 +1496,7 @@ __global__ void __launch_bounds__(256) k_batch_class_scatter(DScene sc, int s, B
     const int i = first + threadIdx.x;
     if (i < n) {
       const int pid = qin[i];
-      const int c = shade_class(sc, ps, pid);
+      const int c = ps.cls[sq->base + i];
       const unsigned int peers = __match_any_sync(__activemask(), c);
       const int leader = __ffs(peers) - 1;
       unsigned int b = 0;

@@ -60,6 +60,7 @@ struct PathState {
   float4* slots;   // [slot][capacity] shadow contributions
   int* queue[2];
   int* binned;           // the queue in shading order
+  uint8_t* cls;          // shading class of each queue position (sort scratch)
   unsigned int* bins;    // class counts and cursors of that order
   float4* shadow_queue;  // 3 float4 per shadow ray
   int* seg;              // batched renders: the segment each path belongs to

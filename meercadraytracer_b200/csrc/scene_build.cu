@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(kBuildBlock) k_bounds(LevelPlan lp, const Slot
 // gives them; lo / scale / live: the binning of each axis.
 __device__ void decide(const Slot& s, const float* nb, const int (*cnt)[kMaxBins], const float (*bbox)[kMaxBins][6],
                        const double* lo, const double* scale, const bool* live, int bins, int j, int* nodes,
-                       Split* split, int* is_split) {
+                       Split* split, int* is_split, bool wide, int* live_out) {
   double best_cost = INFINITY;
   int best_axis = -1, best_split = -1;
   double right_area[kMaxBins];
@@ -356,9 +356,16 @@ __device__ void decide(const Slot& s, const float* nb, const int (*cnt)[kMaxBins
     nd[0] = s.first; nd[1] = s.count; nd[2] = 0;
     split[j] = Split{-1, 0, 0, 0, 0.0, 0.0};
     is_split[j] = 0;
+    live_out[j] = 0;
   } else {
     split[j] = d;
     is_split[j] = 1;
+    // Children that will be leaves whatever the next level decides (few
+    // enough triangles, or at the depth limit) are finished by this node's
+    // scatter when one block partitions it; only the others go on.
+    const bool last = s.depth + 1 >= kBuildDepth;
+    const int small = wide ? 0 : (last || d.nleft <= kMaxLeaf ? 1 : 0) + (last || s.count - d.nleft <= kMaxLeaf ? 1 : 0);
+    live_out[j] = 2 - small;
   }
 }
 
@@ -372,7 +379,7 @@ __global__ void __launch_bounds__(kBuildBlock) k_split(LevelPlan lp, const Slot*
                                                        const float4* __restrict__ cent, float* __restrict__ bounds,
                                                        int* __restrict__ nodes, Split* __restrict__ split,
                                                        int* __restrict__ is_split, WideAcc* __restrict__ acc,
-                                                       int bins) {
+                                                       int bins, int* __restrict__ live_children) {
   __shared__ int sj;
   __shared__ float nb[12];  // node min xyz, -max xyz, centroid min xyz, -max xyz
   __shared__ int cnt[3][kMaxBins];
@@ -404,6 +411,7 @@ __global__ void __launch_bounds__(kBuildBlock) k_split(LevelPlan lp, const Slot*
       nd[0] = s.first; nd[1] = s.count; nd[2] = 0;
       split[j] = Split{-1, 0, 0, 0, 0.0, 0.0};
       is_split[j] = 0;
+      live_children[j] = 0;
     }
     return;
   }
@@ -469,7 +477,7 @@ __global__ void __launch_bounds__(kBuildBlock) k_split(LevelPlan lp, const Slot*
     }
     __syncthreads();
   }
-  if (tid == 0) decide(s, nb, cnt, bbox, lo, scale, live, bins, j, nodes, split, is_split);
+  if (tid == 0) decide(s, nb, cnt, bbox, lo, scale, live, bins, j, nodes, split, is_split, wide, live_children);
 }
 
 // The first triangle of a block's share of its node, and the end.
@@ -524,11 +532,13 @@ __global__ void __launch_bounds__(kBuildBlock) k_count_left(LevelPlan lp, const 
 __global__ void __launch_bounds__(kBuildBlock) k_scatter(LevelPlan lp, const Slot* __restrict__ slots,
                                                          const Split* __restrict__ split,
                                                          const int* __restrict__ rank, int child_base,
-                                                         const uint32_t* __restrict__ order,
+                                                         const uint32_t* order,
                                                          uint32_t* __restrict__ order_out,
                                                          const float4* __restrict__ cent, int* __restrict__ nodes,
                                                          Slot* __restrict__ next, const int* __restrict__ blk_pre,
-                                                         int bins) {
+                                                         int bins, const int* __restrict__ live_pos,
+                                                         uint32_t* order_keep, const float4* __restrict__ bmin,
+                                                         const float4* __restrict__ bmax, float* __restrict__ bounds) {
   using Scan = cub::BlockScan<int, kBuildBlock>;
   __shared__ typename Scan::TempStorage scan_tmp;
   __shared__ int sj;
@@ -567,12 +577,38 @@ __global__ void __launch_bounds__(kBuildBlock) k_scatter(LevelPlan lp, const Slo
     right_off += in_chunk - total;
     __syncthreads();
   }
-  if (tid == 0 && seg == 0) {
+  if (seg != 0) return;
+  if (!wide) __syncthreads();  // this block's order_out writes are visible to thread 0
+  if (tid == 0) {
     const int left = child_base + 2 * rank[j];
     int* nd = nodes + 3 * static_cast<size_t>(s.node);
     nd[0] = left; nd[1] = 0; nd[2] = d.axis;
-    next[2 * rank[j]] = Slot{left, s.first, d.nleft, s.depth + 1};
-    next[2 * rank[j] + 1] = Slot{left + 1, s.first + d.nleft, s.count - d.nleft, s.depth + 1};
+    const Slot kids[2] = {Slot{left, s.first, d.nleft, s.depth + 1},
+                          Slot{left + 1, s.first + d.nleft, s.count - d.nleft, s.depth + 1}};
+    int at = live_pos[j];
+    for (int c = 0; c < 2; c++) {
+      const Slot& k = kids[c];
+      const bool small = !wide && (k.count <= kMaxLeaf || k.depth >= kBuildDepth);
+      if (!small) {
+        next[at++] = k;
+        continue;
+      }
+      // The child is a leaf: its bounds (bvh.ts:55-72 on its triangles) and
+      // node now, and its triangles in both order buffers, since no later
+      // level copies them across.
+      float m[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+      for (int q = k.first; q < k.first + k.count; q++) {
+        const uint32_t t = order_out[q];
+        order_keep[q] = t;
+        const float4 a = bmin[t], b = bmax[t];
+        m[0] = fminf(m[0], a.x); m[1] = fminf(m[1], a.y); m[2] = fminf(m[2], a.z);
+        m[3] = fmaxf(m[3], b.x); m[4] = fmaxf(m[4], b.y); m[5] = fmaxf(m[5], b.z);
+      }
+      float* bo = bounds + 6 * static_cast<size_t>(k.node);
+      for (int a = 0; a < 6; a++) bo[a] = m[a];
+      int* kn = nodes + 3 * static_cast<size_t>(k.node);
+      kn[0] = k.first; kn[1] = k.count; kn[2] = 0;
+    }
   }
 }
 
@@ -805,7 +841,7 @@ struct BuildBuffers {
   DevArray<Slot> slots[2];
   DevArray<Split> split;
   DevArray<int> is_split, rank;
-  DevArray<int> nb, boff, wide, wid, blk_left, blk_pre, totals;
+  DevArray<int> nb, boff, wide, wid, blk_left, blk_pre, totals, live, live_pos;
   DevArray<WideAcc> acc;
   DevArray<uint8_t> scan_tmp;
   DevArray<int> host_pair;
@@ -845,6 +881,8 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
   Split* split = B.split.ensure(max_slots);
   int* is_split = B.is_split.ensure(max_slots);
   int* rank = B.rank.ensure(max_slots);
+  int* live = B.live.ensure(max_slots);
+  int* live_pos = B.live_pos.ensure(max_slots);
   int* nbk = B.nb.ensure(max_slots);
   int* boff = B.boff.ensure(max_slots);
   int* wide = B.wide.ensure(max_slots);
@@ -862,7 +900,7 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
   int active = 1, total = 1, cur = 0;
   uint32_t* order_a = d_order;
   uint32_t* order_b = tmp;
-  int pair[2], tot[2];
+  int pair[2], tot[2], lives[2];
   while (active > 0) {
     k_level_plan<<<blocks_of(active, 256), 256, 0, s>>>(slots[cur], active, nbk, wide);
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, nbk, boff, active, s), "scan");
@@ -877,21 +915,25 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
       k_bounds<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], order_a, bmin, bmax, cent, acc);
     }
     k_split<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], order_a, bmin, bmax, cent, d_bounds, d_nodes, split,
-                                            is_split, acc, bins);
+                                            is_split, acc, bins, live);
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, is_split, rank, active, s), "scan");
+    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, live, live_pos, active, s), "scan");
     check(cudaMemcpyAsync(&pair[0], rank + active - 1, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
     check(cudaMemcpyAsync(&pair[1], is_split + active - 1, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
+    check(cudaMemcpyAsync(&lives[0], live_pos + active - 1, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
+    check(cudaMemcpyAsync(&lives[1], live + active - 1, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
     if (nwide > 0) {
       k_count_left<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], split, order_a, cent, bins, blk_left);
       check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, blk_left, blk_pre, nblocks, s), "scan");
     }
     k_scatter<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], split, rank, total, order_a, order_b, cent, d_nodes,
-                                              slots[cur ^ 1], blk_pre, bins);
+                                              slots[cur ^ 1], blk_pre, bins, live_pos, order_a, bmin, bmax,
+                                              d_bounds);
     check(cudaStreamSynchronize(s), "BVH level");
     const int splits = pair[0] + pair[1];
     std::swap(order_a, order_b);
     total += 2 * splits;
-    active = 2 * splits;
+    active = lives[0] + lives[1];
     cur ^= 1;
     last_levels_++;
   }
