@@ -299,43 +299,76 @@ __global__ void __launch_bounds__(kBuildBlock) k_bounds(LevelPlan lp, const Slot
 __device__ void decide(const Slot& s, const float* nb, const int (*cnt)[kMaxBins], const float (*bbox)[kMaxBins][6],
                        const double* lo, const double* scale, const bool* live, int bins, int j, int* nodes,
                        Split* split, int* is_split, bool wide, int* live_out) {
+  // Called by the 32 lanes of one warp, lane i holding bin i. The right
+  // sweep's unions and counts are suffix scans, the left sweep's prefix
+  // scans (min, max and sums are exact in any order, and the areas and costs
+  // are the same expressions, so every candidate cost equals the one-thread
+  // sweep's); the first minimum in (axis, split) order wins, as there.
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
   double best_cost = INFINITY;
   int best_axis = -1, best_split = -1;
-  double right_area[kMaxBins];
-  int right_count[kMaxBins];
   for (int a = 0; a < 3; a++) {
     if (!live[a]) continue;
-    double rx0 = INFINITY, ry0 = INFINITY, rz0 = INFINITY, rx1 = -INFINITY, ry1 = -INFINITY, rz1 = -INFINITY;
-    int rc = 0;
-    for (int i = bins - 1; i > 0; i--) {
-      const float* o = bbox[a][i];
-      rc += cnt[a][i];
-      rx0 = fmin(rx0, static_cast<double>(o[0])); ry0 = fmin(ry0, static_cast<double>(o[1]));
-      rz0 = fmin(rz0, static_cast<double>(o[2]));
-      rx1 = fmax(rx1, static_cast<double>(o[3])); ry1 = fmax(ry1, static_cast<double>(o[4]));
-      rz1 = fmax(rz1, static_cast<double>(o[5]));
-      right_count[i] = rc;
-      right_area[i] = rc > 0 ? area(rx0, ry0, rz0, rx1, ry1, rz1) : 0;
-    }
-    double lx0 = INFINITY, ly0 = INFINITY, lz0 = INFINITY, lx1 = -INFINITY, ly1 = -INFINITY, lz1 = -INFINITY;
-    int lc = 0;
-    for (int i = 0; i < bins - 1; i++) {
-      const float* o = bbox[a][i];
-      lc += cnt[a][i];
-      lx0 = fmin(lx0, static_cast<double>(o[0])); ly0 = fmin(ly0, static_cast<double>(o[1]));
-      lz0 = fmin(lz0, static_cast<double>(o[2]));
-      lx1 = fmax(lx1, static_cast<double>(o[3])); ly1 = fmax(ly1, static_cast<double>(o[4]));
-      lz1 = fmax(lz1, static_cast<double>(o[5]));
-      const int rc2 = right_count[i + 1];
-      if (lc == 0 || rc2 == 0) continue;
-      const double cost = lc * area(lx0, ly0, lz0, lx1, ly1, lz1) + rc2 * right_area[i + 1];
-      if (cost < best_cost) {
-        best_cost = cost;
-        best_axis = a;
-        best_split = i;
+    const bool in = lane < bins;
+    const float* o = bbox[a][lane < kMaxBins ? lane : 0];
+    int c = in ? cnt[a][lane] : 0;
+    double b0 = in ? static_cast<double>(o[0]) : INFINITY, b1 = in ? static_cast<double>(o[1]) : INFINITY;
+    double b2 = in ? static_cast<double>(o[2]) : INFINITY, b3 = in ? static_cast<double>(o[3]) : -INFINITY;
+    double b4 = in ? static_cast<double>(o[4]) : -INFINITY, b5 = in ? static_cast<double>(o[5]) : -INFINITY;
+    // Suffix: bins [lane, bins).
+    int rc = c;
+    double r0 = b0, r1 = b1, r2 = b2, r3 = b3, r4 = b4, r5 = b5;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int oc = __shfl_down_sync(full, rc, off);
+      const double o0 = __shfl_down_sync(full, r0, off), o1 = __shfl_down_sync(full, r1, off);
+      const double o2 = __shfl_down_sync(full, r2, off), o3 = __shfl_down_sync(full, r3, off);
+      const double o4 = __shfl_down_sync(full, r4, off), o5 = __shfl_down_sync(full, r5, off);
+      if (lane + off < 32) {
+        rc += oc;
+        r0 = fmin(r0, o0); r1 = fmin(r1, o1); r2 = fmin(r2, o2);
+        r3 = fmax(r3, o3); r4 = fmax(r4, o4); r5 = fmax(r5, o5);
       }
     }
+    const double right_area = rc > 0 ? area(r0, r1, r2, r3, r4, r5) : 0;
+    // Prefix: bins [0, lane].
+    int lc = c;
+    double l0 = b0, l1 = b1, l2 = b2, l3 = b3, l4 = b4, l5 = b5;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int oc = __shfl_up_sync(full, lc, off);
+      const double o0 = __shfl_up_sync(full, l0, off), o1 = __shfl_up_sync(full, l1, off);
+      const double o2 = __shfl_up_sync(full, l2, off), o3 = __shfl_up_sync(full, l3, off);
+      const double o4 = __shfl_up_sync(full, l4, off), o5 = __shfl_up_sync(full, l5, off);
+      if (lane >= off) {
+        lc += oc;
+        l0 = fmin(l0, o0); l1 = fmin(l1, o1); l2 = fmin(l2, o2);
+        l3 = fmax(l3, o3); l4 = fmax(l4, o4); l5 = fmax(l5, o5);
+      }
+    }
+    // Split after bin `lane`: the left union with the right union from lane + 1.
+    const int rc2 = __shfl_down_sync(full, rc, 1);
+    const double ra2 = __shfl_down_sync(full, right_area, 1);
+    double cost = INFINITY;
+    if (lane < bins - 1 && lc != 0 && rc2 != 0) {
+      cost = lc * area(l0, l1, l2, l3, l4, l5) + rc2 * ra2;
+      if (isnan(cost)) cost = INFINITY;
+    }
+    int at = lane;
+    for (int off = 16; off > 0; off >>= 1) {
+      const double oc = __shfl_xor_sync(full, cost, off);
+      const int oi = __shfl_xor_sync(full, at, off);
+      if (oc < cost || (oc == cost && oi < at)) {
+        cost = oc;
+        at = oi;
+      }
+    }
+    if (cost < best_cost) {
+      best_cost = cost;
+      best_axis = a;
+      best_split = at;
+    }
   }
+  if (lane != 0) return;
   Split d{1, 0, 0, s.count >> 1, 0.0, 0.0};
   bool leaf = false;
   if (best_axis >= 0) {
@@ -477,7 +510,7 @@ __global__ void __launch_bounds__(kBuildBlock) k_split(LevelPlan lp, const Slot*
     }
     __syncthreads();
   }
-  if (tid == 0) decide(s, nb, cnt, bbox, lo, scale, live, bins, j, nodes, split, is_split, wide, live_children);
+  if (tid < 32) decide(s, nb, cnt, bbox, lo, scale, live, bins, j, nodes, split, is_split, wide, live_children);
 }
 
 // The first triangle of a block's share of its node, and the end.
