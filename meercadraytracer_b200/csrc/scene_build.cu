@@ -40,6 +40,10 @@ constexpr int kBuildBlock = 256;
 // (order independent) atomics, so the decisions equal a single block's.
 constexpr int kWideMin = 1 << 15;
 constexpr int kSegment = 1 << 13;
+// A node of at most kWarpMax triangles is split by one warp (8 per block):
+// a whole block per node left most threads idle at the deep levels.
+constexpr int kWarpMax = 128;
+constexpr int kWarpsPerBlock = kBuildBlock / 32;
 
 void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
@@ -212,21 +216,33 @@ __device__ __forceinline__ int slot_of_block(const LevelPlan& lp, int b) {
 }
 
 // Blocks and wide flag of each slot of a level.
+// Blocks of each slot (0 for a warp-sized node), its wide and small flags.
 __global__ void k_level_plan(const Slot* __restrict__ slots, int active, int* __restrict__ nb,
-                             int* __restrict__ wide) {
+                             int* __restrict__ wide, int* __restrict__ small) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= active) return;
   const int c = slots[j].count;
   const int w = c >= kWideMin ? 1 : 0;
-  nb[j] = w ? (c + kSegment - 1) / kSegment : 1;
+  const int sm = c <= kWarpMax ? 1 : 0;
+  nb[j] = w ? (c + kSegment - 1) / kSegment : (sm ? 0 : 1);
   wide[j] = w;
+  small[j] = sm;
 }
 
 __global__ void k_level_totals(const int* __restrict__ nb, const int* __restrict__ boff,
-                               const int* __restrict__ wide, const int* __restrict__ wid, int active,
+                               const int* __restrict__ wide, const int* __restrict__ wid,
+                               const int* __restrict__ small, const int* __restrict__ spos, int active,
                                int* __restrict__ out) {
   out[0] = boff[active - 1] + nb[active - 1];
   out[1] = wid[active - 1] + wide[active - 1];
+  out[2] = spos[active - 1] + small[active - 1];
+}
+
+// The warp-sized slots of a level, listed.
+__global__ void k_small_list(const int* __restrict__ small, const int* __restrict__ spos, int active,
+                             int* __restrict__ list) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < active && small[j]) list[spos[j]] = j;
 }
 
 __global__ void k_wide_init(WideAcc* __restrict__ acc, int count) {
@@ -513,6 +529,93 @@ __global__ void __launch_bounds__(kBuildBlock) k_split(LevelPlan lp, const Slot*
   if (tid < 32) decide(s, nb, cnt, bbox, lo, scale, live, bins, j, nodes, split, is_split, wide, live_children);
 }
 
+// k_split for warp-sized nodes: one warp per node, 8 per block, with the
+// node's bounds reduced over shuffles and its bins in the warp's own shared
+// memory; the same decisions as a block would take.
+__global__ void __launch_bounds__(kBuildBlock) k_split_small(const int* __restrict__ list, int count,
+                                                             const Slot* __restrict__ slots,
+                                                             const uint32_t* __restrict__ order,
+                                                             const float4* __restrict__ bmin,
+                                                             const float4* __restrict__ bmax,
+                                                             const float4* __restrict__ cent,
+                                                             float* __restrict__ bounds, int* __restrict__ nodes,
+                                                             Split* __restrict__ split, int* __restrict__ is_split,
+                                                             int bins, int* __restrict__ live_children) {
+  __shared__ int cnt_s[kWarpsPerBlock][3][kMaxBins];
+  __shared__ float bbox_s[kWarpsPerBlock][3][kMaxBins][6];
+  const unsigned full = 0xffffffffu;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int k = blockIdx.x * kWarpsPerBlock + w;
+  if (k >= count) return;  // the whole warp
+  const int j = list[k];
+  const Slot s = slots[j];
+  float nb[12];
+  for (int i = 0; i < 12; i++) nb[i] = INFINITY;
+  for (int q = s.first + lane; q < s.first + s.count; q += 32) {
+    const uint32_t t = order[q];
+    const float4 a = bmin[t], b = bmax[t], c = cent[t];
+    nb[0] = fminf(nb[0], a.x); nb[1] = fminf(nb[1], a.y); nb[2] = fminf(nb[2], a.z);
+    nb[3] = fminf(nb[3], -b.x); nb[4] = fminf(nb[4], -b.y); nb[5] = fminf(nb[5], -b.z);
+    nb[6] = fminf(nb[6], c.x); nb[7] = fminf(nb[7], c.y); nb[8] = fminf(nb[8], c.z);
+    nb[9] = fminf(nb[9], -c.x); nb[10] = fminf(nb[10], -c.y); nb[11] = fminf(nb[11], -c.z);
+  }
+  for (int off = 16; off > 0; off >>= 1)
+    for (int i = 0; i < 12; i++) nb[i] = fminf(nb[i], __shfl_xor_sync(full, nb[i], off));
+  if (lane == 0) {
+    float* bo = bounds + 6 * static_cast<size_t>(s.node);
+    bo[0] = nb[0]; bo[1] = nb[1]; bo[2] = nb[2];
+    bo[3] = -nb[3]; bo[4] = -nb[4]; bo[5] = -nb[5];
+  }
+  if (s.count <= kMaxLeaf || s.depth >= kBuildDepth) {
+    if (lane == 0) {
+      int* nd = nodes + 3 * static_cast<size_t>(s.node);
+      nd[0] = s.first; nd[1] = s.count; nd[2] = 0;
+      split[j] = Split{-1, 0, 0, 0, 0.0, 0.0};
+      is_split[j] = 0;
+      live_children[j] = 0;
+    }
+    return;
+  }
+  int (*cnt)[kMaxBins] = cnt_s[w];
+  float (*bbox)[kMaxBins][6] = bbox_s[w];
+  for (int i = lane; i < 3 * kMaxBins; i += 32) {
+    const int a = i / kMaxBins, b = i % kMaxBins;
+    cnt[a][b] = 0;
+    for (int q = 0; q < 3; q++) {
+      bbox[a][b][q] = INFINITY;
+      bbox[a][b][3 + q] = -INFINITY;
+    }
+  }
+  const double cmin[3] = {nb[6], nb[7], nb[8]};
+  const double cmax[3] = {-nb[9], -nb[10], -nb[11]};
+  double lo[3], scale[3];
+  bool live[3];
+  for (int a = 0; a < 3; a++) {
+    lo[a] = cmin[a];
+    const double extent = cmax[a] - lo[a];
+    live[a] = extent > 0;
+    scale[a] = live[a] ? bins / extent : 0.0;
+  }
+  __syncwarp();
+  for (int q = s.first + lane; q < s.first + s.count; q += 32) {
+    const uint32_t t = order[q];
+    const float4 a4 = bmin[t], b4 = bmax[t], c4 = cent[t];
+    for (int a = 0; a < 3; a++) {
+      if (!live[a]) continue;
+      const int b = bin_of(comp4(c4, a), lo[a], scale[a], bins);
+      atomicAdd(&cnt[a][b], 1);
+      atomic_min_f(&bbox[a][b][0], a4.x);
+      atomic_min_f(&bbox[a][b][1], a4.y);
+      atomic_min_f(&bbox[a][b][2], a4.z);
+      atomic_max_f(&bbox[a][b][3], b4.x);
+      atomic_max_f(&bbox[a][b][4], b4.y);
+      atomic_max_f(&bbox[a][b][5], b4.z);
+    }
+  }
+  __syncwarp();
+  decide(s, nb, cnt, bbox, lo, scale, live, bins, j, nodes, split, is_split, false, live_children);
+}
+
 // The first triangle of a block's share of its node, and the end.
 __device__ __forceinline__ void block_range(const Slot& s, bool wide, int seg, int& first, int& end) {
   first = wide ? s.first + seg * kSegment : s.first;
@@ -523,6 +626,44 @@ __device__ __forceinline__ int goes_left(const Split& d, const Slot& s, int k, c
                                          const uint32_t* __restrict__ order, int bins) {
   return d.mode == 0 ? (bin_of(comp4(cent[order[k]], d.axis), d.lo, d.scale, bins) <= d.bin ? 1 : 0)
                      : (k - s.first < d.nleft ? 1 : 0);
+}
+
+// After a split node's partition: its node entry, and its children either
+// queued for the next level (at live_pos[j]) or, when they must be leaves (at
+// most 4 triangles, or at the depth limit; never for a wide parent), finished
+// here: bounds (bvh.ts:55-72 on their triangles), node, and their triangles
+// in both order buffers, since no later level copies them across.
+__device__ void place_children(const Slot& s, const Split& d, bool wide, int j, const int* __restrict__ rank,
+                               int child_base, int* __restrict__ nodes, Slot* __restrict__ next,
+                               const int* __restrict__ live_pos, const uint32_t* order_out, uint32_t* order_keep,
+                               const float4* __restrict__ bmin, const float4* __restrict__ bmax,
+                               float* __restrict__ bounds) {
+  const int left = child_base + 2 * rank[j];
+  int* nd = nodes + 3 * static_cast<size_t>(s.node);
+  nd[0] = left; nd[1] = 0; nd[2] = d.axis;
+  const Slot kids[2] = {Slot{left, s.first, d.nleft, s.depth + 1},
+                        Slot{left + 1, s.first + d.nleft, s.count - d.nleft, s.depth + 1}};
+  int at = live_pos[j];
+  for (int c = 0; c < 2; c++) {
+    const Slot& k = kids[c];
+    const bool small = !wide && (k.count <= kMaxLeaf || k.depth >= kBuildDepth);
+    if (!small) {
+      next[at++] = k;
+      continue;
+    }
+    float m[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    for (int q = k.first; q < k.first + k.count; q++) {
+      const uint32_t t = order_out[q];
+      order_keep[q] = t;
+      const float4 a = bmin[t], b = bmax[t];
+      m[0] = fminf(m[0], a.x); m[1] = fminf(m[1], a.y); m[2] = fminf(m[2], a.z);
+      m[3] = fmaxf(m[3], b.x); m[4] = fmaxf(m[4], b.y); m[5] = fmaxf(m[5], b.z);
+    }
+    float* bo = bounds + 6 * static_cast<size_t>(k.node);
+    for (int a = 0; a < 6; a++) bo[a] = m[a];
+    int* kn = nodes + 3 * static_cast<size_t>(k.node);
+    kn[0] = k.first; kn[1] = k.count; kn[2] = 0;
+  }
 }
 
 // Triangles going left in each block's segment of a wide split node; 0 for
@@ -612,37 +753,53 @@ __global__ void __launch_bounds__(kBuildBlock) k_scatter(LevelPlan lp, const Slo
   }
   if (seg != 0) return;
   if (!wide) __syncthreads();  // this block's order_out writes are visible to thread 0
-  if (tid == 0) {
-    const int left = child_base + 2 * rank[j];
-    int* nd = nodes + 3 * static_cast<size_t>(s.node);
-    nd[0] = left; nd[1] = 0; nd[2] = d.axis;
-    const Slot kids[2] = {Slot{left, s.first, d.nleft, s.depth + 1},
-                          Slot{left + 1, s.first + d.nleft, s.count - d.nleft, s.depth + 1}};
-    int at = live_pos[j];
-    for (int c = 0; c < 2; c++) {
-      const Slot& k = kids[c];
-      const bool small = !wide && (k.count <= kMaxLeaf || k.depth >= kBuildDepth);
-      if (!small) {
-        next[at++] = k;
-        continue;
-      }
-      // The child is a leaf: its bounds (bvh.ts:55-72 on its triangles) and
-      // node now, and its triangles in both order buffers, since no later
-      // level copies them across.
-      float m[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-      for (int q = k.first; q < k.first + k.count; q++) {
-        const uint32_t t = order_out[q];
-        order_keep[q] = t;
-        const float4 a = bmin[t], b = bmax[t];
-        m[0] = fminf(m[0], a.x); m[1] = fminf(m[1], a.y); m[2] = fminf(m[2], a.z);
-        m[3] = fmaxf(m[3], b.x); m[4] = fmaxf(m[4], b.y); m[5] = fmaxf(m[5], b.z);
-      }
-      float* bo = bounds + 6 * static_cast<size_t>(k.node);
-      for (int a = 0; a < 6; a++) bo[a] = m[a];
-      int* kn = nodes + 3 * static_cast<size_t>(k.node);
-      kn[0] = k.first; kn[1] = k.count; kn[2] = 0;
-    }
+  if (tid == 0)
+    place_children(s, d, wide, j, rank, child_base, nodes, next, live_pos, order_out, order_keep, bmin, bmax, bounds);
+}
+
+// k_scatter for warp-sized nodes: one warp per node, a stable partition by
+// ballots over 32-triangle chunks.
+__global__ void __launch_bounds__(kBuildBlock) k_scatter_small(
+    const int* __restrict__ list, int count, const Slot* __restrict__ slots, const Split* __restrict__ split,
+    const int* __restrict__ rank, int child_base, const uint32_t* order, uint32_t* __restrict__ order_out,
+    const float4* __restrict__ cent, int* __restrict__ nodes, Slot* __restrict__ next, int bins,
+    const int* __restrict__ live_pos, uint32_t* order_keep, const float4* __restrict__ bmin,
+    const float4* __restrict__ bmax, float* __restrict__ bounds) {
+  const unsigned full = 0xffffffffu;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int k = blockIdx.x * kWarpsPerBlock + w;
+  if (k >= count) return;  // the whole warp
+  const int j = list[k];
+  const Slot s = slots[j];
+  const Split d = split[j];
+  const int end = s.first + s.count;
+  if (d.mode < 0) {
+    for (int q = s.first + lane; q < end; q += 32) order_out[q] = order[q];
+    return;
   }
+  int left_off = 0, right_off = 0;
+  for (int base = s.first; base < end; base += 32) {
+    const int q = base + lane;
+    int f = 0;
+    uint32_t t = 0;
+    if (q < end) {
+      t = order[q];
+      f = goes_left(d, s, q, cent, order, bins);
+    }
+    const unsigned ballot = __ballot_sync(full, f);
+    const int pre = __popc(ballot & ((1u << lane) - 1u));
+    const int total = __popc(ballot);
+    if (q < end) {
+      const int dst = f ? s.first + left_off + pre : s.first + d.nleft + right_off + (lane - pre);
+      order_out[dst] = t;
+    }
+    left_off += total;
+    right_off += min(32, end - base) - total;
+  }
+  __syncwarp();  // the warp's order_out writes are visible to lane 0
+  if (lane == 0)
+    place_children(s, d, false, j, rank, child_base, nodes, next, live_pos, order_out, order_keep, bmin, bmax,
+                   bounds);
 }
 
 // ---- compile (src/compile.ts:336-343 and 359-432)
@@ -874,7 +1031,7 @@ struct BuildBuffers {
   DevArray<Slot> slots[2];
   DevArray<Split> split;
   DevArray<int> is_split, rank;
-  DevArray<int> nb, boff, wide, wid, blk_left, blk_pre, totals, live, live_pos;
+  DevArray<int> nb, boff, wide, wid, blk_left, blk_pre, totals, live, live_pos, small, spos, slist;
   DevArray<WideAcc> acc;
   DevArray<uint8_t> scan_tmp;
   DevArray<int> host_pair;
@@ -916,13 +1073,16 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
   int* rank = B.rank.ensure(max_slots);
   int* live = B.live.ensure(max_slots);
   int* live_pos = B.live_pos.ensure(max_slots);
+  int* small = B.small.ensure(max_slots);
+  int* spos = B.spos.ensure(max_slots);
+  int* slist = B.slist.ensure(max_slots);
   int* nbk = B.nb.ensure(max_slots);
   int* boff = B.boff.ensure(max_slots);
   int* wide = B.wide.ensure(max_slots);
   int* wid = B.wid.ensure(max_slots);
   int* blk_left = B.blk_left.ensure(max_blocks);
   int* blk_pre = B.blk_pre.ensure(max_blocks);
-  int* totals = B.totals.ensure(2);
+  int* totals = B.totals.ensure(3);
   WideAcc* acc = B.acc.ensure(n / kWideMin + 1);
   k_prepare<<<blocks_of(n, 256), 256, 0, s>>>(d_tris, n, bmin, bmax, cent, d_order);
   Slot root{0, 0, n, 0};
@@ -933,22 +1093,29 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
   int active = 1, total = 1, cur = 0;
   uint32_t* order_a = d_order;
   uint32_t* order_b = tmp;
-  int pair[2], tot[2], lives[2];
+  int pair[2], tot[3], lives[2];
   while (active > 0) {
-    k_level_plan<<<blocks_of(active, 256), 256, 0, s>>>(slots[cur], active, nbk, wide);
+    k_level_plan<<<blocks_of(active, 256), 256, 0, s>>>(slots[cur], active, nbk, wide, small);
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, nbk, boff, active, s), "scan");
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, wide, wid, active, s), "scan");
-    k_level_totals<<<1, 1, 0, s>>>(nbk, boff, wide, wid, active, totals);
+    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, small, spos, active, s), "scan");
+    k_level_totals<<<1, 1, 0, s>>>(nbk, boff, wide, wid, small, spos, active, totals);
+    k_small_list<<<blocks_of(active, 256), 256, 0, s>>>(small, spos, active, slist);
     check(cudaMemcpyAsync(tot, totals, sizeof(tot), cudaMemcpyDeviceToHost, s), "download");
     check(cudaStreamSynchronize(s), "BVH level plan");
-    const int nblocks = tot[0], nwide = tot[1];
+    const int nblocks = tot[0], nwide = tot[1], nsmall = tot[2];
+    const int small_blocks = blocks_of(nsmall, kWarpsPerBlock);
     const LevelPlan lp{nbk, boff, wid, active};
     if (nwide > 0) {
       k_wide_init<<<nwide, 128, 0, s>>>(acc, nwide);
       k_bounds<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], order_a, bmin, bmax, cent, acc);
     }
-    k_split<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], order_a, bmin, bmax, cent, d_bounds, d_nodes, split,
-                                            is_split, acc, bins, live);
+    if (nblocks > 0)
+      k_split<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], order_a, bmin, bmax, cent, d_bounds, d_nodes, split,
+                                              is_split, acc, bins, live);
+    if (nsmall > 0)
+      k_split_small<<<small_blocks, kBuildBlock, 0, s>>>(slist, nsmall, slots[cur], order_a, bmin, bmax, cent,
+                                                         d_bounds, d_nodes, split, is_split, bins, live);
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, is_split, rank, active, s), "scan");
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, live, live_pos, active, s), "scan");
     check(cudaMemcpyAsync(&pair[0], rank + active - 1, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
@@ -959,9 +1126,14 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
       k_count_left<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], split, order_a, cent, bins, blk_left);
       check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, blk_left, blk_pre, nblocks, s), "scan");
     }
-    k_scatter<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], split, rank, total, order_a, order_b, cent, d_nodes,
-                                              slots[cur ^ 1], blk_pre, bins, live_pos, order_a, bmin, bmax,
-                                              d_bounds);
+    if (nblocks > 0)
+      k_scatter<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], split, rank, total, order_a, order_b, cent, d_nodes,
+                                                slots[cur ^ 1], blk_pre, bins, live_pos, order_a, bmin, bmax,
+                                                d_bounds);
+    if (nsmall > 0)
+      k_scatter_small<<<small_blocks, kBuildBlock, 0, s>>>(slist, nsmall, slots[cur], split, rank, total, order_a,
+                                                           order_b, cent, d_nodes, slots[cur ^ 1], bins, live_pos,
+                                                           order_a, bmin, bmax, d_bounds);
     check(cudaStreamSynchronize(s), "BVH level");
     const int splits = pair[0] + pair[1];
     std::swap(order_a, order_b);
