@@ -194,6 +194,33 @@ __global__ void __launch_bounds__(256) k_class_count(DScene sc, PathState ps, co
   if (threadIdx.x < kShadeClasses && h[threadIdx.x]) atomicAdd(&bins[threadIdx.x], h[threadIdx.x]);
 }
 
+// Places the block's tile [first, first + blockDim.x) of the queue: ranks
+// within each warp's class groups, then within the block (shared counters),
+// then one global cursor increment per class and block.
+MCRT_D void scatter_block(const int* __restrict__ queue, const uint8_t* __restrict__ cls, int n, int first,
+                          const unsigned int* base, unsigned int* cursor, int* __restrict__ out) {
+  __shared__ unsigned int blk_count[kShadeClasses], blk_base[kShadeClasses];
+  if (threadIdx.x < kShadeClasses) blk_count[threadIdx.x] = 0;
+  __syncthreads();
+  const int i = first + threadIdx.x;
+  int c = 0, pid = 0;
+  unsigned int pos = 0;
+  if (i < n) {
+    pid = queue[i];
+    c = cls[i];
+    const unsigned int peers = __match_any_sync(__activemask(), c);
+    const int leader = __ffs(peers) - 1;
+    unsigned int w = 0;
+    if (static_cast<int>(threadIdx.x & 31) == leader) w = atomicAdd(&blk_count[c], __popc(peers));
+    pos = __shfl_sync(peers, w, leader) + __popc(peers & lanemask_lt());
+  }
+  __syncthreads();
+  if (threadIdx.x < kShadeClasses && blk_count[threadIdx.x])
+    blk_base[threadIdx.x] = atomicAdd(&cursor[threadIdx.x], blk_count[threadIdx.x]);
+  __syncthreads();
+  if (i < n) out[base[c] + blk_base[c] + pos] = pid;
+}
+
 __global__ void __launch_bounds__(256) k_class_scatter(DScene sc, PathState ps, const int* __restrict__ queue, int n,
                                                        unsigned int* __restrict__ bins, int* __restrict__ out) {
   __shared__ unsigned int base[kShadeClasses];
@@ -204,17 +231,7 @@ __global__ void __launch_bounds__(256) k_class_scatter(DScene sc, PathState ps, 
       sum += bins[b];
     }
   }
-  __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int pid = queue[i];
-  const int c = ps.cls[i];
-  const unsigned int peers = __match_any_sync(__activemask(), c);
-  const int leader = __ffs(peers) - 1;
-  unsigned int b = 0;
-  if (static_cast<int>(threadIdx.x & 31) == leader) b = atomicAdd(&bins[kShadeClasses + c], __popc(peers));
-  b = __shfl_sync(peers, b, leader);
-  out[base[c] + b + __popc(peers & lanemask_lt())] = pid;
+  scatter_block(queue, ps.cls, n, blockIdx.x * blockDim.x, base, bins + kShadeClasses, out);
 }
 
 // ------------------------------------------------------------------- shade
@@ -1493,18 +1510,8 @@ __global__ void __launch_bounds__(256) k_batch_class_scatter(DScene sc, int s, B
   __syncthreads();
   const int stride = gridDim.x * blockDim.x;
   for (int first = blockIdx.x * blockDim.x; first < n; first += stride) {
-    const int i = first + threadIdx.x;
-    if (i < n) {
-      const int pid = qin[i];
-      const int c = ps.cls[sq->base + i];
-      const unsigned int peers = __match_any_sync(__activemask(), c);
-      const int leader = __ffs(peers) - 1;
-      unsigned int b = 0;
-      if (static_cast<int>(threadIdx.x & 31) == leader) b = atomicAdd(&bins[kShadeClasses + c], __popc(peers));
-      b = __shfl_sync(peers, b, leader);
-      out[base[c] + b + __popc(peers & lanemask_lt())] = pid;
-    }
-    __syncwarp();
+    scatter_block(qin, ps.cls + sq->base, n, first, base, bins + kShadeClasses, out);
+    __syncthreads();  // the block's shared counters are reused by the next tile
   }
 }
 
