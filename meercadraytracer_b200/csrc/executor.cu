@@ -103,7 +103,7 @@ __global__ void k_inner_flags(const int* __restrict__ nodes, int m, int* __restr
 __global__ void k_pack_nodes(const float* __restrict__ bounds, const int* __restrict__ nodes,
                              const int* __restrict__ index, int m, DNode* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m || nodes[3 * i + 1] != 0) return;
+  if (i >= m || nodes[3 * i + 1] != 0 || index[i] < 0) return;  // a leaf, or unreachable from the root
   const int l = nodes[3 * i], r = l + 1;
   const float* bl = bounds + 6 * static_cast<size_t>(l);
   const float* br = bounds + 6 * static_cast<size_t>(r);
@@ -553,18 +553,26 @@ int32_t mcrt_send_geometry(mcrt_executor* ex, int32_t version, const mcrt_geomet
       nodes.upload(g->bvh_nodes, sizeof(int) * 3 * m, s);
       k_mark_leaf_ends<<<blocks(m, 256), 256, 0, s>>>(nodes.as<int>(), m, G.tris.as<float4>());
       if (G.root_count == 0) {
-        DevBuf bounds, flag, index, temp;
-        bounds.upload(g->bvh_bounds, sizeof(float) * 6 * m, s);
-        flag.ensure(sizeof(int) * m);
-        index.ensure(sizeof(int) * m);
-        k_inner_flags<<<blocks(m, 256), 256, 0, s>>>(nodes.as<int>(), m, flag.as<int>());
-        size_t temp_bytes = 0;
-        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, flag.as<int>(), index.as<int>(), m, s), "scan");
-        temp.ensure(temp_bytes);
-        cuda_check(cub::DeviceScan::ExclusiveSum(temp.as<void>(), temp_bytes, flag.as<int>(), index.as<int>(), m, s),
-                   "scan");
+        // Inner nodes numbered depth first (preorder, left child first): a
+        // node's left child follows it in memory, often in the same cache
+        // line, and every subtree is one contiguous range.
+        std::vector<int> order_index(m, -1);
+        std::vector<int> todo;
+        todo.reserve(256);
+        todo.push_back(0);
         int inner = 0;
-        for (int i = 0; i < m; i++) inner += g->bvh_nodes[3 * i + 1] == 0;
+        while (!todo.empty()) {
+          const int i = todo.back();
+          todo.pop_back();
+          if (g->bvh_nodes[3 * i + 1] != 0 || order_index[i] >= 0) continue;
+          order_index[i] = inner++;
+          const int first = g->bvh_nodes[3 * i];
+          todo.push_back(first + 1);
+          todo.push_back(first);
+        }
+        DevBuf bounds, index;
+        bounds.upload(g->bvh_bounds, sizeof(float) * 6 * m, s);
+        index.upload(order_index.data(), sizeof(int) * m, s);
         G.nodes.ensure(sizeof(DNode) * std::max(inner, 1));
         k_pack_nodes<<<blocks(m, 256), 256, 0, s>>>(bounds.as<float>(), nodes.as<int>(), index.as<int>(), m,
                                                     G.nodes.as<DNode>());

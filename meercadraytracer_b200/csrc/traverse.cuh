@@ -38,7 +38,7 @@ namespace mcrt {
 constexpr int kShort = 16;  // default shared-memory stack entries per thread
 constexpr int kSentinel = 0x7fffffff;  // empty stack / finished ray
 constexpr int kLeafEnd = 1 << 16;      // in tris[3k].w: last triangle of its leaf
-constexpr int kRefill = 8;             // refill a warp's finished lanes once this many are idle
+constexpr int kRefill = 16;            // refill a warp's finished lanes once this many are idle
 
 // Status bits a kernel reports back (never a trap).
 constexpr unsigned kStatusStackOverflow = 1u;
