@@ -660,6 +660,8 @@ def main() -> None:
     ap.add_argument("--no-large", action="store_true", help="skip the per-frame rebuild workload")
     ap.add_argument("--large-count", type=int, default=4096, help="icospheres of the per-frame rebuild workload")
     ap.add_argument("--large-frames", type=int, default=2, help="timed frames of the per-frame rebuild workload")
+    ap.add_argument("--large-only", action="store_true",
+                    help="run only the per-frame rebuild workload and print its record (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop run")
     ap.add_argument("--batch-capacity", type=int, default=1 << 24, help="path pool of the batch engine")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the served client simulation")
@@ -671,6 +673,9 @@ def main() -> None:
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank)
+    elif args.large_only:
+        if rank == 0:
+            print(json.dumps({"large": run_large(local, args.large_count, args.large_frames)}), flush=True)
     else:
         run_ours(args, rank, world, local)
 

@@ -41,9 +41,13 @@ constexpr int kBuildBlock = 256;
 constexpr int kWideMin = 1 << 15;
 constexpr int kSegment = 1 << 13;
 // A node of at most kWarpMax triangles is split by one warp (8 per block):
-// a whole block per node left most threads idle at the deep levels.
-constexpr int kWarpMax = 128;
+// a whole block per node left most threads idle at the deep levels (512
+// measured 5 % faster than 128 on an 83.9M-triangle build, 2048 no faster).
+constexpr int kWarpMax = 512;
 constexpr int kWarpsPerBlock = kBuildBlock / 32;
+// A node of at most kTinyMax triangles is split by half a warp, one triangle
+// per lane: its bins are never materialised (see k_split_tiny).
+constexpr int kTinyMax = 16;
 
 void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
@@ -215,34 +219,42 @@ __device__ __forceinline__ int slot_of_block(const LevelPlan& lp, int b) {
   return lo;
 }
 
-// Blocks and wide flag of each slot of a level.
-// Blocks of each slot (0 for a warp-sized node), its wide and small flags.
+// Blocks of each slot (0 for a warp- or half-warp-sized node), its wide,
+// small (one warp) and tiny (half a warp) flags.
 __global__ void k_level_plan(const Slot* __restrict__ slots, int active, int* __restrict__ nb,
-                             int* __restrict__ wide, int* __restrict__ small) {
+                             int* __restrict__ wide, int* __restrict__ small, int* __restrict__ tiny) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= active) return;
   const int c = slots[j].count;
   const int w = c >= kWideMin ? 1 : 0;
-  const int sm = c <= kWarpMax ? 1 : 0;
-  nb[j] = w ? (c + kSegment - 1) / kSegment : (sm ? 0 : 1);
+  const int ti = c <= kTinyMax ? 1 : 0;
+  const int sm = !ti && c <= kWarpMax ? 1 : 0;
+  nb[j] = w ? (c + kSegment - 1) / kSegment : (sm || ti ? 0 : 1);
   wide[j] = w;
   small[j] = sm;
+  tiny[j] = ti;
 }
 
 __global__ void k_level_totals(const int* __restrict__ nb, const int* __restrict__ boff,
                                const int* __restrict__ wide, const int* __restrict__ wid,
-                               const int* __restrict__ small, const int* __restrict__ spos, int active,
+                               const int* __restrict__ small, const int* __restrict__ spos,
+                               const int* __restrict__ tiny, const int* __restrict__ tpos, int active,
                                int* __restrict__ out) {
   out[0] = boff[active - 1] + nb[active - 1];
   out[1] = wid[active - 1] + wide[active - 1];
   out[2] = spos[active - 1] + small[active - 1];
+  out[3] = tpos[active - 1] + tiny[active - 1];
 }
 
-// The warp-sized slots of a level, listed.
-__global__ void k_small_list(const int* __restrict__ small, const int* __restrict__ spos, int active,
-                             int* __restrict__ list) {
+// The warp-sized slots of a level, listed, then the half-warp-sized ones
+// (from totals[2] on).
+__global__ void k_small_list(const int* __restrict__ small, const int* __restrict__ spos,
+                             const int* __restrict__ tiny, const int* __restrict__ tpos, int active,
+                             const int* __restrict__ totals, int* __restrict__ list) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < active && small[j]) list[spos[j]] = j;
+  if (j >= active) return;
+  if (small[j]) list[spos[j]] = j;
+  if (tiny[j]) list[totals[2] + tpos[j]] = j;
 }
 
 __global__ void k_wide_init(WideAcc* __restrict__ acc, int count) {
@@ -309,6 +321,43 @@ __global__ void __launch_bounds__(kBuildBlock) k_bounds(LevelPlan lp, const Slot
   if (threadIdx.x < 12) atomic_min_f(&acc[lp.wid[j]].box[threadIdx.x], part[threadIdx.x]);
 }
 
+// The choice of a node (bvh.ts:137-163) from its cheapest split candidate
+// (best_axis < 0: none): a SAH leaf, the binned split with `nleft` triangles
+// on the left, or the median split when the bins put everything on one side.
+__device__ void commit_choice(const Slot& s, const float* nb, double best_cost, int best_axis, int best_split,
+                              int nleft, const double* lo, const double* scale, int j, int* nodes, Split* split,
+                              int* is_split, bool wide, int* live_out) {
+  Split d{1, 0, 0, s.count >> 1, 0.0, 0.0};
+  bool leaf = false;
+  if (best_axis >= 0) {
+    const double parent_area = area(nb[0], nb[1], nb[2], -static_cast<double>(nb[3]), -static_cast<double>(nb[4]),
+                                     -static_cast<double>(nb[5]));
+    const double split_cost = 1 + (1 * best_cost) / fmax(parent_area, 1e-30);
+    if (split_cost >= 1.0 * s.count && s.count <= 16) {
+      leaf = true;
+    } else {
+      d = Split{0, best_axis, best_split, nleft, lo[best_axis], scale[best_axis]};
+      if (nleft == 0 || nleft == s.count) d = Split{1, best_axis, 0, s.count >> 1, 0.0, 0.0};
+    }
+  }
+  if (leaf) {
+    int* nd = nodes + 3 * static_cast<size_t>(s.node);
+    nd[0] = s.first; nd[1] = s.count; nd[2] = 0;
+    split[j] = Split{-1, 0, 0, 0, 0.0, 0.0};
+    is_split[j] = 0;
+    live_out[j] = 0;
+  } else {
+    split[j] = d;
+    is_split[j] = 1;
+    // Children that will be leaves whatever the next level decides (few
+    // enough triangles, or at the depth limit) are finished by this node's
+    // scatter when one block partitions it; only the others go on.
+    const bool last = s.depth + 1 >= kBuildDepth;
+    const int small = wide ? 0 : (last || d.nleft <= kMaxLeaf ? 1 : 0) + (last || s.count - d.nleft <= kMaxLeaf ? 1 : 0);
+    live_out[j] = 2 - small;
+  }
+}
+
 // The SAH sweeps (bvh.ts:110-134) and the choice (bvh.ts:137-163) of one
 // node from its bins, on one thread. nb: the node's 12 bounds as block_bounds
 // gives them; lo / scale / live: the binning of each axis.
@@ -319,7 +368,10 @@ __device__ void decide(const Slot& s, const float* nb, const int (*cnt)[kMaxBins
   // sweep's unions and counts are suffix scans, the left sweep's prefix
   // scans (min, max and sums are exact in any order, and the areas and costs
   // are the same expressions, so every candidate cost equals the one-thread
-  // sweep's); the first minimum in (axis, split) order wins, as there.
+  // sweep's); the first minimum in (axis, split) order wins, as there. The
+  // unions are taken on the float bin bounds and widened to double for the
+  // areas: min and max commute with the exact float-to-double conversion, so
+  // the values are the reference's, for half the shuffles.
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   double best_cost = INFINITY;
@@ -329,36 +381,35 @@ __device__ void decide(const Slot& s, const float* nb, const int (*cnt)[kMaxBins
     const bool in = lane < bins;
     const float* o = bbox[a][lane < kMaxBins ? lane : 0];
     int c = in ? cnt[a][lane] : 0;
-    double b0 = in ? static_cast<double>(o[0]) : INFINITY, b1 = in ? static_cast<double>(o[1]) : INFINITY;
-    double b2 = in ? static_cast<double>(o[2]) : INFINITY, b3 = in ? static_cast<double>(o[3]) : -INFINITY;
-    double b4 = in ? static_cast<double>(o[4]) : -INFINITY, b5 = in ? static_cast<double>(o[5]) : -INFINITY;
+    float b0 = in ? o[0] : INFINITY, b1 = in ? o[1] : INFINITY, b2 = in ? o[2] : INFINITY;
+    float b3 = in ? o[3] : -INFINITY, b4 = in ? o[4] : -INFINITY, b5 = in ? o[5] : -INFINITY;
     // Suffix: bins [lane, bins).
     int rc = c;
-    double r0 = b0, r1 = b1, r2 = b2, r3 = b3, r4 = b4, r5 = b5;
+    float r0 = b0, r1 = b1, r2 = b2, r3 = b3, r4 = b4, r5 = b5;
     for (int off = 1; off < 32; off <<= 1) {
       const int oc = __shfl_down_sync(full, rc, off);
-      const double o0 = __shfl_down_sync(full, r0, off), o1 = __shfl_down_sync(full, r1, off);
-      const double o2 = __shfl_down_sync(full, r2, off), o3 = __shfl_down_sync(full, r3, off);
-      const double o4 = __shfl_down_sync(full, r4, off), o5 = __shfl_down_sync(full, r5, off);
+      const float o0 = __shfl_down_sync(full, r0, off), o1 = __shfl_down_sync(full, r1, off);
+      const float o2 = __shfl_down_sync(full, r2, off), o3 = __shfl_down_sync(full, r3, off);
+      const float o4 = __shfl_down_sync(full, r4, off), o5 = __shfl_down_sync(full, r5, off);
       if (lane + off < 32) {
         rc += oc;
-        r0 = fmin(r0, o0); r1 = fmin(r1, o1); r2 = fmin(r2, o2);
-        r3 = fmax(r3, o3); r4 = fmax(r4, o4); r5 = fmax(r5, o5);
+        r0 = fminf(r0, o0); r1 = fminf(r1, o1); r2 = fminf(r2, o2);
+        r3 = fmaxf(r3, o3); r4 = fmaxf(r4, o4); r5 = fmaxf(r5, o5);
       }
     }
     const double right_area = rc > 0 ? area(r0, r1, r2, r3, r4, r5) : 0;
     // Prefix: bins [0, lane].
     int lc = c;
-    double l0 = b0, l1 = b1, l2 = b2, l3 = b3, l4 = b4, l5 = b5;
+    float l0 = b0, l1 = b1, l2 = b2, l3 = b3, l4 = b4, l5 = b5;
     for (int off = 1; off < 32; off <<= 1) {
       const int oc = __shfl_up_sync(full, lc, off);
-      const double o0 = __shfl_up_sync(full, l0, off), o1 = __shfl_up_sync(full, l1, off);
-      const double o2 = __shfl_up_sync(full, l2, off), o3 = __shfl_up_sync(full, l3, off);
-      const double o4 = __shfl_up_sync(full, l4, off), o5 = __shfl_up_sync(full, l5, off);
+      const float o0 = __shfl_up_sync(full, l0, off), o1 = __shfl_up_sync(full, l1, off);
+      const float o2 = __shfl_up_sync(full, l2, off), o3 = __shfl_up_sync(full, l3, off);
+      const float o4 = __shfl_up_sync(full, l4, off), o5 = __shfl_up_sync(full, l5, off);
       if (lane >= off) {
         lc += oc;
-        l0 = fmin(l0, o0); l1 = fmin(l1, o1); l2 = fmin(l2, o2);
-        l3 = fmax(l3, o3); l4 = fmax(l4, o4); l5 = fmax(l5, o5);
+        l0 = fminf(l0, o0); l1 = fminf(l1, o1); l2 = fminf(l2, o2);
+        l3 = fmaxf(l3, o3); l4 = fmaxf(l4, o4); l5 = fmaxf(l5, o5);
       }
     }
     // Split after bin `lane`: the left union with the right union from lane + 1.
@@ -385,37 +436,10 @@ __device__ void decide(const Slot& s, const float* nb, const int (*cnt)[kMaxBins
     }
   }
   if (lane != 0) return;
-  Split d{1, 0, 0, s.count >> 1, 0.0, 0.0};
-  bool leaf = false;
-  if (best_axis >= 0) {
-    const double parent_area = area(nb[0], nb[1], nb[2], -static_cast<double>(nb[3]), -static_cast<double>(nb[4]),
-                                     -static_cast<double>(nb[5]));
-    const double split_cost = 1 + (1 * best_cost) / fmax(parent_area, 1e-30);
-    if (split_cost >= 1.0 * s.count && s.count <= 16) {
-      leaf = true;
-    } else {
-      int nleft = 0;
-      for (int i = 0; i <= best_split; i++) nleft += cnt[best_axis][i];
-      d = Split{0, best_axis, best_split, nleft, lo[best_axis], scale[best_axis]};
-      if (nleft == 0 || nleft == s.count) d = Split{1, best_axis, 0, s.count >> 1, 0.0, 0.0};
-    }
-  }
-  if (leaf) {
-    int* nd = nodes + 3 * static_cast<size_t>(s.node);
-    nd[0] = s.first; nd[1] = s.count; nd[2] = 0;
-    split[j] = Split{-1, 0, 0, 0, 0.0, 0.0};
-    is_split[j] = 0;
-    live_out[j] = 0;
-  } else {
-    split[j] = d;
-    is_split[j] = 1;
-    // Children that will be leaves whatever the next level decides (few
-    // enough triangles, or at the depth limit) are finished by this node's
-    // scatter when one block partitions it; only the others go on.
-    const bool last = s.depth + 1 >= kBuildDepth;
-    const int small = wide ? 0 : (last || d.nleft <= kMaxLeaf ? 1 : 0) + (last || s.count - d.nleft <= kMaxLeaf ? 1 : 0);
-    live_out[j] = 2 - small;
-  }
+  int nleft = 0;
+  if (best_axis >= 0)
+    for (int i = 0; i <= best_split; i++) nleft += cnt[best_axis][i];
+  commit_choice(s, nb, best_cost, best_axis, best_split, nleft, lo, scale, j, nodes, split, is_split, wide, live_out);
 }
 
 // Bounds, leaf test, binning and SAH choice of every node of a level
@@ -614,6 +638,140 @@ __global__ void __launch_bounds__(kBuildBlock) k_split_small(const int* __restri
   }
   __syncwarp();
   decide(s, nb, cnt, bbox, lo, scale, live, bins, j, nodes, split, is_split, false, live_children);
+}
+
+// k_split for nodes of at most kTinyMax triangles: half a warp per node, one
+// triangle per lane, so two nodes per warp. Per axis the lanes sort their
+// triangles by bin (a bitonic network on bin * 16 + lane), then prefix and
+// suffix unions over the sorted order give, at the last triangle of each
+// occupied bin b, the left set {bins <= b} and the right set {bins > b} of the
+// split after b. Split positions between occupied bins have the same two sets
+// and so the same cost as the occupied bin before them, and positions before
+// the first or from the last occupied bin leave a side empty, so the first
+// minimum over these candidates in (axis, split) order is the binned sweep's:
+// the same costs from the same float unions, the same choice.
+__global__ void __launch_bounds__(kBuildBlock) k_split_tiny(const int* __restrict__ list, int count,
+                                                            const Slot* __restrict__ slots,
+                                                            const uint32_t* __restrict__ order,
+                                                            const float4* __restrict__ bmin,
+                                                            const float4* __restrict__ bmax,
+                                                            const float4* __restrict__ cent,
+                                                            float* __restrict__ bounds, int* __restrict__ nodes,
+                                                            Split* __restrict__ split, int* __restrict__ is_split,
+                                                            int bins, int* __restrict__ live_children) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, i = lane & 15;
+  const int pair = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  if (2 * pair >= count) return;  // the whole warp
+  const int k = 2 * pair + (lane >> 4);
+  const bool valid = k < count;  // this half holds a node (every lane still shuffles)
+  const int j = valid ? list[k] : 0;
+  const Slot s = valid ? slots[j] : Slot{0, 0, 0, 0};
+  const int n = s.count;
+  const bool has = i < n;
+  float m[12];
+  for (int q = 0; q < 12; q++) m[q] = INFINITY;
+  float4 a4 = make_float4(INFINITY, INFINITY, INFINITY, 0.0f), b4 = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
+  float4 c4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (has) {
+    const uint32_t t = order[s.first + i];
+    a4 = bmin[t];
+    b4 = bmax[t];
+    c4 = cent[t];
+    m[0] = a4.x; m[1] = a4.y; m[2] = a4.z;
+    m[3] = -b4.x; m[4] = -b4.y; m[5] = -b4.z;
+    m[6] = c4.x; m[7] = c4.y; m[8] = c4.z;
+    m[9] = -c4.x; m[10] = -c4.y; m[11] = -c4.z;
+  }
+  for (int off = 8; off > 0; off >>= 1)
+    for (int q = 0; q < 12; q++) m[q] = fminf(m[q], __shfl_xor_sync(full, m[q], off, 16));
+  const bool leafy = n <= kMaxLeaf || s.depth >= kBuildDepth;
+  if (valid && i == 0) {
+    float* bo = bounds + 6 * static_cast<size_t>(s.node);
+    bo[0] = m[0]; bo[1] = m[1]; bo[2] = m[2];
+    bo[3] = -m[3]; bo[4] = -m[4]; bo[5] = -m[5];
+    if (leafy) {
+      int* nd = nodes + 3 * static_cast<size_t>(s.node);
+      nd[0] = s.first; nd[1] = s.count; nd[2] = 0;
+      split[j] = Split{-1, 0, 0, 0, 0.0, 0.0};
+      is_split[j] = 0;
+      live_children[j] = 0;
+    }
+  }
+  const bool work = valid && !leafy;
+  double lo[3], scale[3];
+  bool live[3];
+  for (int a = 0; a < 3; a++) {
+    lo[a] = m[6 + a];
+    const double extent = -static_cast<double>(m[9 + a]) - lo[a];
+    live[a] = work && extent > 0;
+    scale[a] = live[a] ? bins / extent : 0.0;
+  }
+  double best_cost = INFINITY;
+  int best_axis = -1, best_split = -1, best_nleft = 0;
+  for (int a = 0; a < 3; a++) {
+    // Sort the half's triangles by bin; lanes without one sort last.
+    const int bin = (has && live[a]) ? bin_of(comp4(c4, a), lo[a], scale[a], bins) : kMaxBins;
+    int key = (bin << 4) | i;
+    for (int kk = 2; kk <= 16; kk <<= 1) {
+      for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+        const int other = __shfl_xor_sync(full, key, jj, 16);
+        const bool keep_min = ((i & jj) == 0) == ((i & kk) == 0);
+        key = keep_min ? min(key, other) : max(key, other);
+      }
+    }
+    const int src = key & 15, sb = key >> 4;
+    float l0 = __shfl_sync(full, a4.x, src, 16), l1 = __shfl_sync(full, a4.y, src, 16);
+    float l2 = __shfl_sync(full, a4.z, src, 16), l3 = __shfl_sync(full, b4.x, src, 16);
+    float l4 = __shfl_sync(full, b4.y, src, 16), l5 = __shfl_sync(full, b4.z, src, 16);
+    float r0 = l0, r1 = l1, r2 = l2, r3 = l3, r4 = l4, r5 = l5;
+    for (int off = 1; off < 16; off <<= 1) {
+      const float o0 = __shfl_up_sync(full, l0, off, 16), o1 = __shfl_up_sync(full, l1, off, 16);
+      const float o2 = __shfl_up_sync(full, l2, off, 16), o3 = __shfl_up_sync(full, l3, off, 16);
+      const float o4 = __shfl_up_sync(full, l4, off, 16), o5 = __shfl_up_sync(full, l5, off, 16);
+      if (i >= off) {
+        l0 = fminf(l0, o0); l1 = fminf(l1, o1); l2 = fminf(l2, o2);
+        l3 = fmaxf(l3, o3); l4 = fmaxf(l4, o4); l5 = fmaxf(l5, o5);
+      }
+      const float p0 = __shfl_down_sync(full, r0, off, 16), p1 = __shfl_down_sync(full, r1, off, 16);
+      const float p2 = __shfl_down_sync(full, r2, off, 16), p3 = __shfl_down_sync(full, r3, off, 16);
+      const float p4 = __shfl_down_sync(full, r4, off, 16), p5 = __shfl_down_sync(full, r5, off, 16);
+      if (i + off < 16) {
+        r0 = fminf(r0, p0); r1 = fminf(r1, p1); r2 = fminf(r2, p2);
+        r3 = fmaxf(r3, p3); r4 = fmaxf(r4, p4); r5 = fmaxf(r5, p5);
+      }
+    }
+    // Split after bin sb (this lane the last of its bin): positions [0, i] left, (i, n) right.
+    const double right_here = i < n ? area(r0, r1, r2, r3, r4, r5) : 0;
+    const double right_area = __shfl_down_sync(full, right_here, 1, 16);
+    const int next_bin = __shfl_down_sync(full, sb, 1, 16);
+    double cost = INFINITY;
+    const int lc = i + 1, rc = n - i - 1;
+    if (live[a] && i < n - 1 && sb != next_bin) {
+      cost = lc * area(l0, l1, l2, l3, l4, l5) + rc * right_area;
+      if (isnan(cost)) cost = INFINITY;
+    }
+    int at = sb, atl = lc;
+    for (int off = 8; off > 0; off >>= 1) {
+      const double oc = __shfl_xor_sync(full, cost, off, 16);
+      const int oi = __shfl_xor_sync(full, at, off, 16);
+      const int ol = __shfl_xor_sync(full, atl, off, 16);
+      if (oc < cost || (oc == cost && oi < at)) {
+        cost = oc;
+        at = oi;
+        atl = ol;
+      }
+    }
+    if (cost < best_cost) {
+      best_cost = cost;
+      best_axis = a;
+      best_split = at;
+      best_nleft = atl;
+    }
+  }
+  if (work && i == 0)
+    commit_choice(s, m, best_cost, best_axis, best_split, best_nleft, lo, scale, j, nodes, split, is_split, false,
+                  live_children);
 }
 
 // The first triangle of a block's share of its node, and the end.
@@ -1031,7 +1189,7 @@ struct BuildBuffers {
   DevArray<Slot> slots[2];
   DevArray<Split> split;
   DevArray<int> is_split, rank;
-  DevArray<int> nb, boff, wide, wid, blk_left, blk_pre, totals, live, live_pos, small, spos, slist;
+  DevArray<int> nb, boff, wide, wid, blk_left, blk_pre, totals, live, live_pos, small, spos, tiny, tpos, slist;
   DevArray<WideAcc> acc;
   DevArray<uint8_t> scan_tmp;
   DevArray<int> host_pair;
@@ -1075,6 +1233,8 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
   int* live_pos = B.live_pos.ensure(max_slots);
   int* small = B.small.ensure(max_slots);
   int* spos = B.spos.ensure(max_slots);
+  int* tiny = B.tiny.ensure(max_slots);
+  int* tpos = B.tpos.ensure(max_slots);
   int* slist = B.slist.ensure(max_slots);
   int* nbk = B.nb.ensure(max_slots);
   int* boff = B.boff.ensure(max_slots);
@@ -1082,7 +1242,7 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
   int* wid = B.wid.ensure(max_slots);
   int* blk_left = B.blk_left.ensure(max_blocks);
   int* blk_pre = B.blk_pre.ensure(max_blocks);
-  int* totals = B.totals.ensure(3);
+  int* totals = B.totals.ensure(4);
   WideAcc* acc = B.acc.ensure(n / kWideMin + 1);
   k_prepare<<<blocks_of(n, 256), 256, 0, s>>>(d_tris, n, bmin, bmax, cent, d_order);
   Slot root{0, 0, n, 0};
@@ -1093,18 +1253,21 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
   int active = 1, total = 1, cur = 0;
   uint32_t* order_a = d_order;
   uint32_t* order_b = tmp;
-  int pair[2], tot[3], lives[2];
+  int pair[2], tot[4], lives[2];
   while (active > 0) {
-    k_level_plan<<<blocks_of(active, 256), 256, 0, s>>>(slots[cur], active, nbk, wide, small);
+    k_level_plan<<<blocks_of(active, 256), 256, 0, s>>>(slots[cur], active, nbk, wide, small, tiny);
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, nbk, boff, active, s), "scan");
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, wide, wid, active, s), "scan");
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, small, spos, active, s), "scan");
-    k_level_totals<<<1, 1, 0, s>>>(nbk, boff, wide, wid, small, spos, active, totals);
-    k_small_list<<<blocks_of(active, 256), 256, 0, s>>>(small, spos, active, slist);
+    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, tiny, tpos, active, s), "scan");
+    k_level_totals<<<1, 1, 0, s>>>(nbk, boff, wide, wid, small, spos, tiny, tpos, active, totals);
+    k_small_list<<<blocks_of(active, 256), 256, 0, s>>>(small, spos, tiny, tpos, active, totals, slist);
     check(cudaMemcpyAsync(tot, totals, sizeof(tot), cudaMemcpyDeviceToHost, s), "download");
     check(cudaStreamSynchronize(s), "BVH level plan");
-    const int nblocks = tot[0], nwide = tot[1], nsmall = tot[2];
+    const int nblocks = tot[0], nwide = tot[1], nsmall = tot[2], ntiny = tot[3];
     const int small_blocks = blocks_of(nsmall, kWarpsPerBlock);
+    // Both lists share k_scatter_small, one warp per node.
+    const int scatter_blocks = blocks_of(nsmall + ntiny, kWarpsPerBlock);
     const LevelPlan lp{nbk, boff, wid, active};
     if (nwide > 0) {
       k_wide_init<<<nwide, 128, 0, s>>>(acc, nwide);
@@ -1116,6 +1279,9 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
     if (nsmall > 0)
       k_split_small<<<small_blocks, kBuildBlock, 0, s>>>(slist, nsmall, slots[cur], order_a, bmin, bmax, cent,
                                                          d_bounds, d_nodes, split, is_split, bins, live);
+    if (ntiny > 0)
+      k_split_tiny<<<blocks_of(ntiny, 2 * kWarpsPerBlock), kBuildBlock, 0, s>>>(
+          slist + nsmall, ntiny, slots[cur], order_a, bmin, bmax, cent, d_bounds, d_nodes, split, is_split, bins, live);
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, is_split, rank, active, s), "scan");
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, live, live_pos, active, s), "scan");
     check(cudaMemcpyAsync(&pair[0], rank + active - 1, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
@@ -1130,8 +1296,8 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
       k_scatter<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], split, rank, total, order_a, order_b, cent, d_nodes,
                                                 slots[cur ^ 1], blk_pre, bins, live_pos, order_a, bmin, bmax,
                                                 d_bounds);
-    if (nsmall > 0)
-      k_scatter_small<<<small_blocks, kBuildBlock, 0, s>>>(slist, nsmall, slots[cur], split, rank, total, order_a,
+    if (nsmall + ntiny > 0)
+      k_scatter_small<<<scatter_blocks, kBuildBlock, 0, s>>>(slist, nsmall + ntiny, slots[cur], split, rank, total, order_a,
                                                            order_b, cent, d_nodes, slots[cur ^ 1], bins, live_pos,
                                                            order_a, bmin, bmax, d_bounds);
     check(cudaStreamSynchronize(s), "BVH level");
