@@ -861,7 +861,7 @@ __global__ void __launch_bounds__(B) k_shadow(DScene sc, PathState ps, int n, in
   st.sp = 0;
   unsigned status = 0;
   ShadowQuery q{sc, ps, capacity, &status};
-  traverse_persistent(sc, q, n, &cnt->fetch, st, status);
+  traverse_persistent(sc, q, n, &cnt->fetch_shadow, st, status);
   if (status) atomicOr(&cnt->status, status);
 }
 
@@ -1049,7 +1049,23 @@ __global__ void __launch_bounds__(kBlock) k_count_hits(DScene sc, const float4* 
 }
 
 // ------------------------------------------------------------------- host
-PathBuffers::~PathBuffers() { release(); }
+PathBuffers::~PathBuffers() {
+  release();
+  if (fork_) cudaEventDestroy(fork_);
+  if (join_) cudaEventDestroy(join_);
+  if (side_) cudaStreamDestroy(side_);
+}
+
+cudaError_t PathBuffers::side_stream(cudaStream_t* side, cudaEvent_t* fork, cudaEvent_t* join) {
+  cudaError_t e = cudaSuccess;
+  if (!side_) e = cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !fork_) e = cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming);
+  if (e == cudaSuccess && !join_) e = cudaEventCreateWithFlags(&join_, cudaEventDisableTiming);
+  *side = side_;
+  *fork = fork_;
+  *join = join_;
+  return e;
+}
 
 void PathBuffers::release() {
   for (void* p : allocations_) cudaFree(p);
@@ -1242,6 +1258,27 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
   RenderStats local;
   RenderStats& st = stats ? *stats : local;
   cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(Counters), stream);
+  // Untimed renders trace bounce k's shadow rays and resolve its paths on a
+  // side stream while bounce k + 1's closest hits (and shading sort) run on
+  // the main one: neither touches what the other reads or writes, and each
+  // fills the other's tail of idle SMs. Shading k + 1 waits for the side
+  // stream (it rewrites the shadow queue, the slots and the path queue that
+  // resolve reads). Timed renders keep one stream, so every kernel's events
+  // bracket it alone.
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  bool overlap = !timed;
+  if (overlap && e == cudaSuccess) {
+    e = buffers.side_stream(&side, &fork, &join);
+    overlap = e == cudaSuccess;
+  }
+  bool side_busy = false;  // side work queued since the main stream last joined it
+  auto join_side = [&]() {
+    if (side_busy) {
+      cudaStreamWaitEvent(stream, join, 0);
+      side_busy = false;
+    }
+  };
   for (int first = 0; first < passes && e == cudaSuccess; first += chunk_passes) {
     const int np = std::min(chunk_passes, passes - first);
     int n = np * npix;
@@ -1266,7 +1303,6 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
       tv.extend<<<persistent_blocks(tv.extend, n, tv.block), tv.block, 0, stream>>>(scene, ps, ps.queue[cur], n, cnt);
       tm.stop(st.ms_extend, st.n_extend);
       st.closest_rays += n;
-      cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), stream);
       const int* shade_queue = ps.queue[cur];
       if (sort_shading && n >= kSortMin) {
         cudaMemsetAsync(ps.bins, 0, 2 * kShadeClasses * sizeof(unsigned int), stream);
@@ -1275,6 +1311,8 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
         shade_queue = ps.binned;
         st.launches += 2;
       }
+      join_side();
+      cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), stream);
       tm.start();
       k_shade<<<blocks_for(n, kBlock), kBlock, 0, stream>>>(scene, f, ps, shade_queue, n, ps.queue[cur ^ 1], cnt);
       tm.stop(st.ms_shade, st.n_shade);
@@ -1284,28 +1322,44 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
       const int n_next = static_cast<int>(host->next_count);
       const int n_shadow = static_cast<int>(host->shadow_count);
       st.status |= host->status;
+      cudaStream_t sh = stream;
+      if (overlap) {
+        cudaEventRecord(fork, stream);
+        cudaStreamWaitEvent(side, fork, 0);
+        sh = side;
+      }
       if (n_shadow > 0) {
-        cudaMemsetAsync(&cnt->fetch, 0, sizeof(unsigned int), stream);
+        cudaMemsetAsync(&cnt->fetch_shadow, 0, sizeof(unsigned int), sh);
         tm.start();
-        tv.shadow<<<persistent_blocks(tv.shadow, n_shadow, tv.block), tv.block, 0, stream>>>(scene, ps, n_shadow, cap,
-                                                                                             cnt);
+        tv.shadow<<<persistent_blocks(tv.shadow, n_shadow, tv.block), tv.block, 0, sh>>>(scene, ps, n_shadow, cap,
+                                                                                         cnt);
         tm.stop(st.ms_shadow, st.n_shadow);
         st.any_rays += n_shadow;
         st.launches++;
       }
       tm.start();
-      k_resolve<<<blocks_for(n, kBlock), kBlock, 0, stream>>>(scene, f, ps, ps.queue[cur], n, cap);
+      k_resolve<<<blocks_for(n, kBlock), kBlock, 0, sh>>>(scene, f, ps, ps.queue[cur], n, cap);
       tm.stop(st.ms_resolve, st.n_resolve);
+      if (overlap) {
+        cudaEventRecord(join, side);
+        side_busy = true;
+      }
       st.launches += 3;
       n = n_next;
       cur ^= 1;
     }
+    join_side();
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess && on_chunk) {
       tm.start();
       e = on_chunk(ctx, first, np);
       tm.stop(st.ms_accumulate, st.n_accumulate);
     }
+  }
+  join_side();
+  if (side) {
+    const cudaError_t es = cudaStreamSynchronize(side);
+    if (e == cudaSuccess) e = es;
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
   if (e == cudaSuccess) {

@@ -70,7 +70,8 @@ struct Counters {
   unsigned int next_count;
   unsigned int shadow_count;
   unsigned int status;
-  unsigned int fetch;  // next query a persistent traversal warp takes
+  unsigned int fetch;         // next query a closest-hit traversal warp takes
+  unsigned int fetch_shadow;  // the same for the any-hit (shadow) traversal
 };
 
 // Work and time of the kernels of one render, for benchmarks.
@@ -96,9 +97,14 @@ class PathBuffers {
   size_t bytes() const { return bytes_; }
   Counters* counters() const { return counters_; }
   Counters* host_counters() const { return host_counters_; }
+  // A second stream and two events (made on first use, kept until destruction)
+  // for running a bounce's shadow rays beside the next bounce's closest hits.
+  cudaError_t side_stream(cudaStream_t* side, cudaEvent_t* fork, cudaEvent_t* join);
 
  private:
   void release();
+  cudaStream_t side_ = nullptr;
+  cudaEvent_t fork_ = nullptr, join_ = nullptr;
   PathState st_{};
   Counters* counters_ = nullptr;
   Counters* host_counters_ = nullptr;
