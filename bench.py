@@ -344,6 +344,8 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                    "compile_s": {"flatten_host": round(t_flat, 3), "gpu_bvh_compile": round(t_build, 3),
                                  "upload": round(t_upload, 3)}},
         "wall_s_timed": round(wall, 3),
+        # Camera samples (pixels x spp) per second over all ranks, the second figure of the metric.
+        "samples_per_s": round(w * h * spp * world / (device_ms / args.steps / 1e3)),
         "gpu_launches": launches,
         "clocks": clk,
         "e2e": e2e,

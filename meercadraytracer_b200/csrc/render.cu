@@ -303,20 +303,12 @@ MCRT_D void direct_light(const FrameParams& fp, const DScene& sc, ShadowEmitter&
 
 // One iteration of samplePixel's loop for path `pid`.
 MCRT_D void shade_path(const DScene& sc, const FrameParams& fp, const PathState& ps, int pid, const StageQueues& qs) {
-  const float4 o4 = ps.ray_o[pid], d4 = ps.ray_d[pid], h4 = ps.hit[pid];
-  float4 T4 = ps.thr[pid], L4 = ps.rad[pid];
+  // The hit word and flags first: a miss (most camera rays of open scenes)
+  // reads little more, so the rest of the path state is loaded after the test.
+  const float4 h4 = ps.hit[pid];
   uint32_t fl = ps.flags[pid];
-  uint32_t rng = ps.rng[pid];
-  V3 d = V3{d4.x, d4.y, d4.z};
-  V3 T = V3{T4.x, T4.y, T4.z};
-  V3 Lr = V3{L4.x, L4.y, L4.z};
-  float fog_factor = T4.w;
-  float last_env_scale = L4.w;
-  ShadowEmitter em{qs.shadow, qs.shadow_count, pid, 0ull};
   const unsigned word = __float_as_uint(h4.w);
   const int tri = static_cast<int>(word & 0x7fffffffu) - 1;
-  const bool front = (word & 0x80000000u) != 0;
-  const float inf = __int_as_float(0x7f800000);
 
   if (tri < 0) {
     if (!(fl & kFlagSeen)) {
@@ -340,7 +332,8 @@ MCRT_D void shade_path(const DScene& sc, const FrameParams& fp, const PathState&
           c[2] = t.z * bg.intensity;
           srgb_tex = sc.textures[bg.texture].srgb;
         } else {
-          V3 e = sample_environment(sc, bg.environment, d);
+          const float4 d4 = ps.ray_d[pid];
+          V3 e = sample_environment(sc, bg.environment, V3{d4.x, d4.y, d4.z});
           c[0] = e.x;
           c[1] = e.y;
           c[2] = e.z;
@@ -354,19 +347,33 @@ MCRT_D void shade_path(const DScene& sc, const FrameParams& fp, const PathState&
         out = make_float4(fp.clear_color[0] * a, fp.clear_color[1] * a, fp.clear_color[2] * a, a);
       }
       ps.sample[pid] = out;
-      fl |= kFlagDone | kFlagDirect;
-    } else {
-      const int le = flag_last_env(fl);
-      if (le >= 0) {
-        V3 e = sample_environment(sc, le, d);
-        Lr = Lr + T * e * last_env_scale;
-      }
-      fl |= kFlagDone;
+      ps.flags[pid] = fl | kFlagDone | kFlagDirect;  // the radiance is left as it is
+      return;
     }
-    ps.rad[pid] = make_float4(Lr.x, Lr.y, Lr.z, last_env_scale);
-    ps.flags[pid] = fl;
+    const float4 L4 = ps.rad[pid];
+    V3 Lr = V3{L4.x, L4.y, L4.z};
+    const int le = flag_last_env(fl);
+    if (le >= 0) {
+      const float4 d4 = ps.ray_d[pid], T4 = ps.thr[pid];
+      V3 e = sample_environment(sc, le, V3{d4.x, d4.y, d4.z});
+      Lr = Lr + V3{T4.x, T4.y, T4.z} * e * L4.w;
+    }
+    ps.rad[pid] = make_float4(Lr.x, Lr.y, Lr.z, L4.w);
+    ps.flags[pid] = fl | kFlagDone;
     return;
   }
+
+  const float4 o4 = ps.ray_o[pid], d4 = ps.ray_d[pid];
+  float4 T4 = ps.thr[pid], L4 = ps.rad[pid];
+  uint32_t rng = ps.rng[pid];
+  V3 d = V3{d4.x, d4.y, d4.z};
+  V3 T = V3{T4.x, T4.y, T4.z};
+  V3 Lr = V3{L4.x, L4.y, L4.z};
+  float fog_factor = T4.w;
+  float last_env_scale = L4.w;
+  ShadowEmitter em{qs.shadow, qs.shadow_count, pid, 0ull};
+  const bool front = (word & 0x80000000u) != 0;
+  const float inf = __int_as_float(0x7f800000);
 
   const float t = h4.x;
   const float4 m4 = ps.med[pid];
