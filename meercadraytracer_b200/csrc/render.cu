@@ -108,9 +108,9 @@ MCRT_D void raygen_path(const FrameParams& fp, const PathState& ps, int pid) {
                               static_cast<float>(near_[2]), 0.0f);
   ps.ray_d[pid] = make_float4(static_cast<float>(dx / len), static_cast<float>(dy / len),
                               static_cast<float>(dz / len), 0.0f);
-  ps.thr[pid] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-  ps.rad[pid] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-  ps.med[pid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  // Throughput, radiance and medium are not written here: until its first
+  // shaded hit (kFlagSeen) a path's are always (1, 1, 1, fog 0), (0, 0, 0,
+  // env scale 1) and no medium, which shade_path uses without loading them.
   ps.rng[pid] = rng;
   ps.flags[pid] = kFlagToneMap | kFlagCull;
   ps.smask[pid] = 0ull;
@@ -364,7 +364,14 @@ MCRT_D void shade_path(const DScene& sc, const FrameParams& fp, const PathState&
   }
 
   const float4 o4 = ps.ray_o[pid], d4 = ps.ray_d[pid];
-  float4 T4 = ps.thr[pid], L4 = ps.rad[pid];
+  const bool seen = (fl & kFlagSeen) != 0;
+  float4 T4 = make_float4(1.0f, 1.0f, 1.0f, 0.0f), L4 = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+  float4 m4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (seen) {
+    T4 = ps.thr[pid];
+    L4 = ps.rad[pid];
+    m4 = ps.med[pid];
+  }
   uint32_t rng = ps.rng[pid];
   V3 d = V3{d4.x, d4.y, d4.z};
   V3 T = V3{T4.x, T4.y, T4.z};
@@ -376,7 +383,6 @@ MCRT_D void shade_path(const DScene& sc, const FrameParams& fp, const PathState&
   const float inf = __int_as_float(0x7f800000);
 
   const float t = h4.x;
-  const float4 m4 = ps.med[pid];
   if (m4.x > 0.0f || m4.y > 0.0f || m4.z > 0.0f) {
     // Beer-Lambert absorption inside the volume, tracer.ts:128-131.
     T.x *= expf(-m4.x * t);
@@ -430,11 +436,12 @@ MCRT_D void shade_path(const DScene& sc, const FrameParams& fp, const PathState&
       qs.next[queue_append(qs.next_count)] = pid;
     }
     ps.thr[pid] = make_float4(T.x, T.y, T.z, fog_factor);
+    if (!seen) ps.rad[pid] = L4;  // read by resolve if the path ends here
     ps.rng[pid] = rng;
     ps.flags[pid] = fl;
     return;
   }
-  if (!(fl & kFlagSeen)) {
+  if (!seen) {
     fl |= kFlagSeen;
     if (!mat.tone_mapped) fl &= ~kFlagToneMap;
     // fog, tracer.ts:649-656.
@@ -876,6 +883,7 @@ __global__ void __launch_bounds__(B) k_shadow(DScene sc, PathState ps, int n, in
 // Adds the path's shadowed light; tone maps and fogs a finished path.
 MCRT_D void resolve_path(const DScene& sc, const FrameParams& fp, const PathState& ps, int pid, int capacity) {
   const uint32_t fl = ps.flags[pid];
+  if (fl & kFlagDirect) return;  // a background sample, written by shading; no shadow rays
   unsigned long long mask = ps.smask[pid];
   if (mask == 0ull && !(fl & kFlagDone)) return;
   float4 L4 = ps.rad[pid];
@@ -892,7 +900,6 @@ MCRT_D void resolve_path(const DScene& sc, const FrameParams& fp, const PathStat
     ps.rad[pid] = L4;
     return;
   }
-  if (fl & kFlagDirect) return;
   // Tone map and fog the finished path, tracer.ts:472-477.
   float c[3] = {L4.x, L4.y, L4.z};
   if ((fl & kFlagToneMap) && fp.tone_mapping != 0) tone_map(c, fp.tone_mapping, fp.exposure);
