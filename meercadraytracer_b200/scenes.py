@@ -4,7 +4,7 @@ No public dataset is involved: every scene is generated from a fixed seed
 (0x5EED0000 + configuration index) with the shapes, sizes and value
 distributions the configurations name. Placements the configurations leave
 open (light positions, camera of the mid scene, ground material) are fixed
-here and documented in DESIGN.md.
+here, in the functions below.
 
   small_scene()  22,530 triangles: a 40 x 40 ground plane and 64 UV spheres
                  (16 x 12 segments), 320 x 240, 16 spp, GI off, ACES, sRGB.
