@@ -205,6 +205,27 @@ def test_gpu_render_is_deterministic(gpu, small):
     assert np.array_equal(a, c)
 
 
+def test_gpu_two_stream_render_equals_one_stream_render():
+    # Untimed renders trace each bounce's shadow rays on a second stream beside the
+    # next bounce's closest hits; timed renders keep one stream. GI on, several
+    # bounces and a path pool of 32,768 (one pass per chunk), so every overlap case occurs.
+    b = scenes.mid_scene(grid=4, width=160, height=120, samples=8)
+    compiled = compile_scene(b.scene, builder=cpu.compile_sink)
+    cam = compile_camera(b.camera)
+    st = trace_settings(as_options(b.options))
+    ex = GpuExecutor(0)
+    try:
+        ex.set_capacity(1 << 15)
+        ex.set_timing(True)
+        one = ex.raytrace(compiled, cam, b.width, b.height, st, 8, True)
+        ex.set_timing(False)
+        two = ex.raytrace(compiled, cam, b.width, b.height, st, 8, True)
+        assert ex.stats()["path_bytes"] < 64 << 20  # the small pool was used
+    finally:
+        ex.dispose()
+    assert np.array_equal(one, two)
+
+
 def test_gpu_render_pixels_match_full_render(gpu, small):
     b, compiled, cam = small
     st = trace_settings(as_options(b.options))
