@@ -1232,7 +1232,7 @@ struct PlainVariant {
 
 #define MCRT_PLAIN_VARIANT(B, S) PlainVariant{B, S, k_extend<B, S>, k_shadow<B, S>}
 const PlainVariant kPlainVariants[] = {
-    MCRT_PLAIN_VARIANT(128, 16), MCRT_PLAIN_VARIANT(64, 16), MCRT_PLAIN_VARIANT(128, 8),
+    MCRT_PLAIN_VARIANT(128, 8), MCRT_PLAIN_VARIANT(64, 16), MCRT_PLAIN_VARIANT(128, 16),
     MCRT_PLAIN_VARIANT(128, 24), MCRT_PLAIN_VARIANT(256, 8), MCRT_PLAIN_VARIANT(256, 16),
 };
 #undef MCRT_PLAIN_VARIANT
@@ -1675,7 +1675,7 @@ struct BatchVariant {
 // The same variants, in the same order, as kPlainVariants.
 #define MCRT_BATCH_VARIANT(B, S) BatchVariant{B, S, k_batch_extend<B, S>, k_batch_shadow<B, S>}
 const BatchVariant kBatchVariants[] = {
-    MCRT_BATCH_VARIANT(128, 16), MCRT_BATCH_VARIANT(64, 16), MCRT_BATCH_VARIANT(128, 8),
+    MCRT_BATCH_VARIANT(128, 8), MCRT_BATCH_VARIANT(64, 16), MCRT_BATCH_VARIANT(128, 16),
     MCRT_BATCH_VARIANT(128, 24), MCRT_BATCH_VARIANT(256, 8), MCRT_BATCH_VARIANT(256, 16),
 };
 #undef MCRT_BATCH_VARIANT
