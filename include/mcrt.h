@@ -240,7 +240,7 @@ int32_t mcrt_set_capacity(mcrt_executor* executor, int32_t paths);
 
 /* The traversal kernel variants compiled into the library: up to `max`
  * (threads per block, shared-memory short-stack entries per thread) pairs,
- * and *count = how many there are. Variant 0, (128, 8), is the default. No
+ * and *count = how many there are. Variant 0, (128, 4), is the default. No
  * counterpart in the reference (its traversal is one JavaScript loop). */
 int32_t mcrt_traversal_variants(int32_t max, int32_t* blocks, int32_t* stacks, int32_t* count);
 

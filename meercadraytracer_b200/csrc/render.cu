@@ -1232,8 +1232,8 @@ struct PlainVariant {
 
 #define MCRT_PLAIN_VARIANT(B, S) PlainVariant{B, S, k_extend<B, S>, k_shadow<B, S>}
 const PlainVariant kPlainVariants[] = {
-    MCRT_PLAIN_VARIANT(128, 8), MCRT_PLAIN_VARIANT(64, 16), MCRT_PLAIN_VARIANT(128, 16),
-    MCRT_PLAIN_VARIANT(128, 24), MCRT_PLAIN_VARIANT(256, 8), MCRT_PLAIN_VARIANT(256, 16),
+    MCRT_PLAIN_VARIANT(128, 4), MCRT_PLAIN_VARIANT(128, 8), MCRT_PLAIN_VARIANT(64, 16),
+    MCRT_PLAIN_VARIANT(128, 16), MCRT_PLAIN_VARIANT(256, 8), MCRT_PLAIN_VARIANT(256, 16),
 };
 #undef MCRT_PLAIN_VARIANT
 constexpr int kVariantCount = static_cast<int>(sizeof(kPlainVariants) / sizeof(kPlainVariants[0]));
@@ -1675,8 +1675,8 @@ struct BatchVariant {
 // The same variants, in the same order, as kPlainVariants.
 #define MCRT_BATCH_VARIANT(B, S) BatchVariant{B, S, k_batch_extend<B, S>, k_batch_shadow<B, S>}
 const BatchVariant kBatchVariants[] = {
-    MCRT_BATCH_VARIANT(128, 8), MCRT_BATCH_VARIANT(64, 16), MCRT_BATCH_VARIANT(128, 16),
-    MCRT_BATCH_VARIANT(128, 24), MCRT_BATCH_VARIANT(256, 8), MCRT_BATCH_VARIANT(256, 16),
+    MCRT_BATCH_VARIANT(128, 4), MCRT_BATCH_VARIANT(128, 8), MCRT_BATCH_VARIANT(64, 16),
+    MCRT_BATCH_VARIANT(128, 16), MCRT_BATCH_VARIANT(256, 8), MCRT_BATCH_VARIANT(256, 16),
 };
 #undef MCRT_BATCH_VARIANT
 static_assert(sizeof(kBatchVariants) / sizeof(kBatchVariants[0]) == kVariantCount, "variant tables differ");
