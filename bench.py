@@ -381,7 +381,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                                           f"{base['seconds']:.1f} s) of the same workload on the oracle, a C++ "
                                           f"restatement of the reference's TypeScript path (no Node.js here)"}
     if world == 1 and not args.no_large:
-        line["large"] = run_large(local, args.large_count, args.large_frames)
+        line["large"] = run_large(local, args.large_count, args.large_frames, tune=not args.no_tune)
     if world == 1 and not (args.no_batch and args.no_serve):
         # The batched and served forms of the same path, beside the plain number.
         from meercadraytracer_b200 import scenes as SC
@@ -559,11 +559,12 @@ def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: 
 
 
 # ------------------------------------------------------ per-frame rebuild
-def run_large(device: int, count: int, frames: int, bins: int = 32) -> Dict[str, Any]:
+def run_large(device: int, count: int, frames: int, bins: int = 32, tune: bool = True) -> Dict[str, Any]:
     """The large workload: `count` icospheres (20,480 triangles each) under rigid transforms
     re-drawn every frame; each frame compiles the instances on the GPU (flatten, binned-SAH
     BVH with `bins` bins, reorder, tangents) and renders 2048 x 2048 at 16 spp, GI on,
-    8 bounces. Two untimed warm-up frames first (allocations)."""
+    8 bounces. Two untimed warm-up frames first (allocations); with `tune`, the second
+    traces once per traversal variant and the fastest is kept for the timed frames."""
     import torch
 
     from meercadraytracer_b200 import scenes as SC
@@ -583,11 +584,23 @@ def run_large(device: int, count: int, frames: int, bins: int = 32) -> Dict[str,
         image = torch.empty(L.width * L.height * 4, dtype=torch.uint8, device=f"cuda:{device}")
         rows = []
         warm = 2
+        variant_ms: Dict[str, float] = {}
         for k in range(frames + warm):
             t0 = time.perf_counter()
             instances = L.frame(k)
             t_host = time.perf_counter() - t0
             info, _ = ex.compile_instances(instances, bins=bins)
+            if tune and k == warm - 1:
+                from meercadraytracer_b200._lib import traversal_variants
+
+                for b_, s_ in traversal_variants():
+                    ex.set_traversal(b_, s_)
+                    ex.reset_stats()
+                    ex.raytrace_resident((info["version"], sv), cam, L.width, L.height, st, spp, srgb,
+                                         device_ptr=image.data_ptr())
+                    variant_ms[f"{b_}x{s_}"] = round(ex.stats()["ms_total"], 1)
+                best = min(variant_ms, key=variant_ms.get)
+                ex.set_traversal(*(int(x) for x in best.split("x")))
             ex.reset_stats()
             ex.raytrace_resident((info["version"], sv), cam, L.width, L.height, st, spp, srgb,
                                  device_ptr=image.data_ptr())
@@ -604,8 +617,12 @@ def run_large(device: int, count: int, frames: int, bins: int = 32) -> Dict[str,
                          "rays": int(rays), "levels": info["levels"], "nodes": info["node_count"],
                          "hbm_bytes": {"geometry": int(info["geometry_bytes"]), "builder": int(info["build_bytes"]),
                                        "path_state": int(s["path_bytes"]), "device_used_by_process": int(free0 - free1)}})
-        return {"workload": L.name, "triangles": L.triangles, "bins": bins, "leaf_size": 4, "frames": rows,
-                "hbm_total_bytes": int(total_mem)}
+        out = {"workload": L.name, "triangles": L.triangles, "bins": bins, "leaf_size": 4, "frames": rows,
+               "hbm_total_bytes": int(total_mem)}
+        if variant_ms:
+            out["traversal_variant_ms"] = variant_ms
+            out["traversal_variant"] = min(variant_ms, key=variant_ms.get)
+        return out
     finally:
         ex.dispose()
 
@@ -677,7 +694,7 @@ def main() -> None:
         run_reference(args, rank)
     elif args.large_only:
         if rank == 0:
-            print(json.dumps({"large": run_large(local, args.large_count, args.large_frames)}), flush=True)
+            print(json.dumps({"large": run_large(local, args.large_count, args.large_frames, tune=not args.no_tune)}), flush=True)
     else:
         run_ours(args, rank, world, local)
 
