@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(B, 1280 / B) k_extend(DScene sc, PathState ps,
   st.sp = 0;
   unsigned status = 0;
   ExtendQuery q{sc, ps, queue, 0, {}};
-  traverse_persistent(sc, q, n, &cnt->fetch, st, status);
+  traverse_persistent<kRefillClosest>(sc, q, n, &cnt->fetch, st, status);
   if (status) atomicOr(&cnt->status, status);
 }
 
@@ -877,7 +877,7 @@ __global__ void __launch_bounds__(B) k_shadow(DScene sc, PathState ps, int n, in
   st.sp = 0;
   unsigned status = 0;
   ShadowQuery q{sc, ps, capacity, &status};
-  traverse_persistent(sc, q, n, &cnt->fetch_shadow, st, status);
+  traverse_persistent<kRefillShadow>(sc, q, n, &cnt->fetch_shadow, st, status);
   if (status) atomicOr(&cnt->status, status);
 }
 
@@ -1473,7 +1473,7 @@ __global__ void __launch_bounds__(B) k_batch_extend(DScene sc, int s, BatchTable
   st.sp = 0;
   unsigned status = 0;
   ExtendQuery q{sc, ps, ps.queue[t->iteration & 1] + sq->base, 0, {}};
-  traverse_persistent(sc, q, n, &sq->fetch, st, status);
+  traverse_persistent<kRefillClosest>(sc, q, n, &sq->fetch, st, status);
   if (status) atomicOr(&bc->status, status);
 }
 
@@ -1520,7 +1520,7 @@ __global__ void __launch_bounds__(B) k_batch_shadow(DScene sc, int s, BatchTable
   PathState pq = ps;
   pq.shadow_queue += 3ull * sq->base * static_cast<unsigned>(slots);
   ShadowQuery q{sc, pq, capacity, &status};
-  traverse_persistent(sc, q, n, &sq->fetch_shadow, st, status);
+  traverse_persistent<kRefillShadow>(sc, q, n, &sq->fetch_shadow, st, status);
   if (status) atomicOr(&bc->status, status);
 }
 

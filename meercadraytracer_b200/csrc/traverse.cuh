@@ -39,6 +39,10 @@ constexpr int kShort = 16;  // default shared-memory stack entries per thread
 constexpr int kSentinel = 0x7fffffff;  // empty stack / finished ray
 constexpr int kLeafEnd = 1 << 16;      // in tris[3k].w: last triangle of its leaf
 constexpr int kRefill = 16;            // refill a warp's finished lanes once this many are idle
+// The same threshold for the render's own kernels, measured on the mid workload
+// (closest hits: 12 of 8, 12, 16, 20; shadow rays: 20).
+constexpr int kRefillClosest = 12;
+constexpr int kRefillShadow = 20;
 
 // Status bits a kernel reports back (never a trap).
 constexpr unsigned kStatusStackOverflow = 1u;
@@ -209,7 +213,8 @@ MCRT_D int root_ref(const DScene& sc) { return sc.root_count > 0 ? ~0 : 0; }
 //   bool leaf(int first)      test the leaf starting at triangle `first`;
 //                             false ends the query (any hit: blocked)
 //   void finish()             write the query's result
-template <class Q, class ST>
+// REFILL: a warp takes new queries once that many of its lanes are idle.
+template <int REFILL = kRefill, class Q, class ST>
 MCRT_D void traverse_persistent(const DScene& sc, Q& q, int n, unsigned* counter, ST& st,
                                 unsigned& status) {
   const unsigned lane = threadIdx.x & 31;
@@ -305,7 +310,7 @@ MCRT_D void traverse_persistent(const DScene& sc, Q& q, int n, unsigned* counter
         q.finish();
         has = false;
       }
-    } while (__popc(__ballot_sync(0xffffffffu, !has)) < kRefill && __any_sync(0xffffffffu, has));
+    } while (__popc(__ballot_sync(0xffffffffu, !has)) < REFILL && __any_sync(0xffffffffu, has));
   }
 }
 
