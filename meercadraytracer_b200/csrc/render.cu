@@ -1464,7 +1464,7 @@ __global__ void __launch_bounds__(kBlock) k_batch_raygen(const BatchTables* __re
 }
 
 template <int B, int S>
-__global__ void __launch_bounds__(B) k_batch_extend(DScene sc, int s, BatchTables* t, PathState ps,
+__global__ void __launch_bounds__(B, 1280 / B) k_batch_extend(DScene sc, int s, BatchTables* t, PathState ps,
                                                     BatchCounters* bc) {
   SceneQueues* sq = &t->scenes[s];
   const int n = static_cast<int>(sq->count);
