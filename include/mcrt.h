@@ -6,7 +6,7 @@
  * the TileExecutor interface of src/executors.ts:4-14). It keeps the latest
  * geometry and shading it was sent, by version, and texture pixels by id, all
  * resident in HBM, and renders tiles or whole images from them. A Node-API
- * addon (or any FFI) binds these functions one to one; see INTEGRATION.md.
+ * addon (or any FFI) binds these functions one to one.
  *
  * Conventions: every function returns MCRT_OK (0) or an error code, and
  * mcrt_last_error() then returns the message (per thread). Host pointers are
@@ -30,6 +30,8 @@ extern "C" {
 #define MCRT_ERR_NO_SCENE 3  /* geometry / shading version not received */
 #define MCRT_ERR_TEXTURE 4   /* a texture id was not sent */
 #define MCRT_ERR_LIMIT 5     /* beyond a documented limit */
+#define MCRT_ERR_WALK 6      /* a BVH walk reached one of its bounds (mcrt_stats.status
+                                bits), so the result may differ from the reference's */
 
 typedef struct mcrt_executor mcrt_executor;
 
@@ -44,7 +46,10 @@ typedef struct mcrt_stats {
   uint64_t n_raygen, n_extend, n_shade, n_shadow, n_resolve, n_accumulate;
   uint64_t path_bytes;    /* HBM held for path state */
   uint64_t scene_bytes;   /* HBM held for the resident scene */
-  uint32_t status;        /* kernel-reported limits hit: 1 stack, 2 shadow list */
+  uint32_t status;        /* bounds BVH walks reached (each also fails its call with
+                             MCRT_ERR_WALK): 1 traversal stack deeper than 104 entries,
+                             2 more than 64 distinct see-through hits on one shadow ray,
+                             4 a query's step budget, 8 a leaf past the last triangle */
   uint32_t pad_;
 } mcrt_stats;
 
@@ -250,6 +255,11 @@ int32_t mcrt_traversal_variants(int32_t max, int32_t* blocks, int32_t* stacks, i
 int32_t mcrt_set_traversal(mcrt_executor* executor, int32_t block, int32_t stack);
 
 int32_t mcrt_get_stats(mcrt_executor* executor, mcrt_stats* out);
+/* Test and debugging hook: caps the node visits plus leaves one BVH query may
+ * take (a walk of a well-formed tree of N triangles takes fewer than 2N + 64,
+ * the default, restored by 0). A query that reaches the cap ends, sets status
+ * bit 4 and its call fails with MCRT_ERR_WALK. */
+int32_t mcrt_set_step_limit(mcrt_executor* executor, int32_t steps);
 int32_t mcrt_reset_stats(mcrt_executor* executor);
 
 /* ------------------------------------------------------------------------

@@ -17,6 +17,7 @@ MCRT_ERR_CUDA = 2
 MCRT_ERR_NO_SCENE = 3
 MCRT_ERR_TEXTURE = 4
 MCRT_ERR_LIMIT = 5
+MCRT_ERR_WALK = 6  # a BVH walk reached a bound (stack depth, see-through list, step budget)
 
 # Rays per call of mcrt_intersect_closest_noalloc (its fixed per-device array holds this many).
 NOALLOC_MAX_RAYS = 1 << 16
@@ -28,6 +29,11 @@ class McrtError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(message)
         self.code = code
+
+
+class WalkLimitError(McrtError):
+    """A call whose BVH walks reached one of their bounds (MCRT_ERR_WALK): its result
+    may differ from the reference's, so none is returned."""
 
 
 class mcrt_stats(C.Structure):
@@ -93,6 +99,7 @@ SIGNATURES = {
     "mcrt_batch_set_traversal": (_i32, [_vp, _i32, _i32]),
     "mcrt_get_stats": (_i32, [_vp, _P(mcrt_stats)]),
     "mcrt_reset_stats": (_i32, [_vp]),
+    "mcrt_set_step_limit": (_i32, [_vp, _i32]),
 }
 
 _lib: Optional[C.CDLL] = None
@@ -119,7 +126,8 @@ def call(name: str, *args) -> None:
     lib = load()
     code = getattr(lib, name)(*args)
     if code != MCRT_OK:
-        raise McrtError(code, lib.mcrt_last_error().decode(errors="replace") or f"{name} failed ({code})")
+        message = lib.mcrt_last_error().decode(errors="replace") or f"{name} failed ({code})"
+        raise (WalkLimitError if code == MCRT_ERR_WALK else McrtError)(code, message)
 
 
 def traversal_variants() -> list:

@@ -6,7 +6,7 @@ input is the host-side object model. The per-triangle flatten (addMesh,
 src/compile.ts:212-306) is vectorised with numpy into "sink" arrays. What
 follows it -- BVH build, reorder into BVH order, tangents and epsilon
 (src/compile.ts:327-432) -- is done by a geometry builder: the product's is the
-GPU one in `geometry_builder.py`.
+GPU one, `GpuExecutor.compile_sink` (libmcrt's `mcrt_compile_geometry`).
 """
 from __future__ import annotations
 
@@ -76,6 +76,38 @@ def collect_objects(scene: S.Scene, filter: Optional[Callable[[Any], bool]] = No
     return meshes, lights
 
 
+_IDENTITY3 = (1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0)
+
+
+def _texture_pixels(texture: Any, data: Any) -> np.ndarray:
+    """readImage's decode of one RGBA image (src/textures.ts:60-110): 8-bit data
+    kept, half floats widened, anything else as float32."""
+    data = np.asarray(data)
+    channels = data.size // max(1, texture.width * texture.height)
+    if channels != 4:
+        raise ValueError("only RGBA data textures are supported")
+    if texture.type == S.HalfFloatType:
+        data = data.astype(np.uint16).view(np.float16).astype(np.float32)
+    elif data.dtype != np.uint8:
+        data = data.astype(np.float32)
+    return data.reshape(-1)
+
+
+def _to_compiled(texture: Any, pixels: np.ndarray, flip_y: bool, matrix: Sequence[float]) -> CompiledTexture:
+    """toCompiled, src/textures.ts:113-127."""
+    srgb = pixels.dtype == np.uint8 and texture.color_space == S.SRGBColorSpace
+    return CompiledTexture(texture.width, texture.height, pixels, bool(srgb), bool(flip_y), texture.wrap_s,
+                           texture.wrap_t, tuple(matrix))
+
+
+class _Face:
+    """The source of one cube face in the texture table: its pixel array, which
+    identifies the face when pixels are shipped to an executor."""
+
+    def __init__(self, data: Any) -> None:
+        self.data = data
+
+
 class TextureTable:
     """TextureTable, src/textures.ts:134-198: each texture stored once."""
 
@@ -84,43 +116,60 @@ class TextureTable:
         self.environments: List[CompiledEnvironment] = []
         self.keys: List[Any] = []  # source object of each texture, for identity-based ids
         self._index: Dict[int, int] = {}
+        self._environment_index: Dict[Tuple[Any, ...], int] = {}
 
     def add(self, texture: Optional[S.DataTexture]) -> int:
-        if texture is None:
+        """add, src/textures.ts:141-157: a material map or screen background; cube
+        textures are environments only."""
+        if texture is None or isinstance(texture, S.CubeTexture):
             return -1
         key = id(texture)
         if key in self._index:
             return self._index[key]
-        data = np.asarray(texture.data)
-        channels = data.size // max(1, texture.width * texture.height)
-        if channels != 4:
-            raise ValueError("only RGBA data textures are supported")
-        if texture.type == S.HalfFloatType:
-            data = data.astype(np.uint16).view(np.float16).astype(np.float32)
-        elif data.dtype != np.uint8:
-            data = data.astype(np.float32)
-        srgb = data.dtype == np.uint8 and texture.color_space == S.SRGBColorSpace
         index = len(self.textures)
-        self.textures.append(CompiledTexture(texture.width, texture.height, data.reshape(-1), srgb,
-                                             bool(texture.flip_y), texture.wrap_s, texture.wrap_t,
-                                             texture.matrix()))
+        self.textures.append(_to_compiled(texture, _texture_pixels(texture, texture.data), bool(texture.flip_y),
+                                          texture.matrix()))
         self.keys.append(texture)
         self._index[key] = index
         return index
 
     def add_environment(self, texture: Any, intensity: float, rotation: Any) -> int:
-        """addEnvironment, src/textures.ts:164-197, for equirectangular data textures."""
+        """addEnvironment, src/textures.ts:164-197: cube textures (six faces, x
+        mirrored unless a render target) and equirectangular textures, each
+        (texture, version, intensity, rotation) compiled once."""
         if texture is None:
             return -1
         matrix = _euler_to_matrix_transposed(rotation)
-        if texture.mapping in (S.EquirectangularReflectionMapping, S.EquirectangularRefractionMapping):
+        key = (id(texture), getattr(texture, "version", 0), float(intensity), tuple(matrix))
+        if key in self._environment_index:
+            return self._environment_index[key]
+        environment: Optional[CompiledEnvironment] = None
+        mapping = texture.mapping
+        if isinstance(texture, S.CubeTexture) or mapping in (S.CubeReflectionMapping, S.CubeRefractionMapping):
+            images = list(getattr(texture, "images", []))
+            faces: List[int] = []
+            if len(images) == 6:
+                for image in images:
+                    self.textures.append(_to_compiled(texture, _texture_pixels(texture, image), False, _IDENTITY3))
+                    self.keys.append(_Face(image))
+                    faces.append(len(self.textures) - 1)
+            if len(faces) == 6:
+                environment = CompiledEnvironment("cube", matrix, float(intensity), faces=tuple(faces),
+                                                  flip_x=not getattr(texture, "is_render_target_texture", False))
+            else:
+                warn_once("a cube texture without six readable images is ignored")
+        elif mapping in (S.EquirectangularReflectionMapping, S.EquirectangularRefractionMapping):
             index = self.add(texture)
-            if index < 0:
-                return -1
-            self.environments.append(CompiledEnvironment("equirect", matrix, float(intensity), texture=index))
-            return len(self.environments) - 1
-        warn_once(f"environment textures with mapping {texture.mapping} are not supported and are ignored")
-        return -1
+            if index >= 0:
+                environment = CompiledEnvironment("equirect", matrix, float(intensity), texture=index)
+        else:
+            warn_once(f"environment textures with mapping {mapping} are not supported and are ignored")
+        index = -1
+        if environment is not None:
+            self.environments.append(environment)
+            index = len(self.environments) - 1
+        self._environment_index[key] = index
+        return index
 
 
 def _euler_to_matrix_transposed(euler: Any) -> Tuple[float, ...]:
@@ -157,7 +206,7 @@ def compile_material(m: S.Material, table: TextureTable) -> CompiledMaterial:
     env_map = -1
     if m.env_map is not None:
         env_map = table.add_environment(m.env_map, m.env_map_intensity if m.env_map_intensity is not None else 1,
-                                        None)
+                                        getattr(m, "env_map_rotation", None))
     emissive = m.emissive.tuple(m.emissive_intensity) if m.emissive is not None else (0.0, 0.0, 0.0)
     return CompiledMaterial(
         model=model,
@@ -232,8 +281,8 @@ def compile_background(scene: S.Scene, table: TextureTable) -> CompiledBackgroun
         return CompiledBackground("clear")
     if isinstance(bg, S.Color):
         return CompiledBackground("color", color=bg.tuple())
-    if isinstance(bg, S.DataTexture):
-        if bg.mapping in (301, 302, 303, 304):
+    if isinstance(bg, (S.DataTexture, S.CubeTexture)):
+        if isinstance(bg, S.CubeTexture) or bg.mapping in (301, 302, 303, 304):
             env = table.add_environment(bg, scene.background_intensity, scene.background_rotation)
             return CompiledBackground("environment", environment=env, intensity=scene.background_intensity) \
                 if env >= 0 else CompiledBackground("clear")
@@ -456,10 +505,11 @@ GeometryBuilder = Callable[[TriangleSink], CompiledGeometry]
 
 
 def default_builder() -> GeometryBuilder:
-    """The product's geometry builder: GPU BVH build, reorder, tangents and epsilon."""
-    from .geometry_builder import build_geometry_gpu
+    """The product's geometry builder: BVH build, reorder, tangents and epsilon on the
+    GPU, through the default executor's `compile_sink`."""
+    from .executors import default_executor
 
-    return build_geometry_gpu
+    return lambda sink: default_executor().compile_sink(sink)
 
 
 def compile_geometry(meshes: Sequence[S.Mesh], material_index: Callable[[Any], int],

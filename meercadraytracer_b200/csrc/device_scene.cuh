@@ -98,6 +98,7 @@ struct DScene {
   cudaTextureObject_t dfg;   // 512 floats: (scale, bias) per texel
   int light_count;
   int environment;           // scene.environment, or -1
+  int step_limit;            // > 0: node visits plus leaves one query may take (a test hook)
   DBackground background;
   DFog fog;
 };

@@ -204,6 +204,7 @@ struct mcrt_executor {
   PathBuffers paths;
   int capacity = 1 << 24;  // paths in flight: 16M, about 9 GB of path state with 5 lights
   int variant = 0;         // traversal kernels' (block, short stack) variant
+  int step_limit = 0;      // > 0: a query's step budget (mcrt_set_step_limit)
   bool timed = false;
   RenderStats stats;
   double ms_total = 0;
@@ -222,6 +223,23 @@ namespace {
 void download(mcrt_executor* ex, void* host, const void* dev, size_t bytes, const char* what) {
   cuda_check(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, ex->stream), what);
   cuda_check(cudaStreamSynchronize(ex->stream), what);
+}
+
+// Fails the call with MCRT_ERR_WALK when its BVH walks reached a bound: the
+// reference's walks have none (src/bvh.ts:202-332, src/tracer.ts:515-594), so
+// the result may differ from the reference's and is not handed back as valid,
+// as the reference's worker reports any failure ({type: 'error'},
+// src/protocol.ts:101-104).
+void check_walk(unsigned status) {
+  status &= kStatusStackOverflow | kStatusShadowListOverflow | kStatusStepLimit | kStatusLeafRange;
+  if (!status) return;
+  std::string m = "a BVH walk reached a bound, so the result may differ from the reference's:";
+  if (status & kStatusStackOverflow) m += " traversal stack deeper than " + std::to_string(kStackMax) + " entries;";
+  if (status & kStatusShadowListOverflow) m += " more than 64 distinct see-through hits on one shadow ray;";
+  if (status & kStatusStepLimit) m += " a query's step budget ran out;";
+  if (status & kStatusLeafRange) m += " a leaf ran past the last triangle;";
+  m.pop_back();
+  fail(MCRT_ERR_WALK, m);
 }
 
 double half_to_double(unsigned h) {  // halfToFloat, src/color.ts:28-35
@@ -260,6 +278,7 @@ DScene make_scene(mcrt_executor* ex) {
   s.dfg = ex->dfg_tex;
   s.light_count = ex->sh.light_count;
   s.environment = ex->sh.environment;
+  s.step_limit = ex->step_limit;
   s.background = ex->sh.background;
   s.fog = ex->sh.fog;
   return s;
@@ -337,19 +356,27 @@ void run_frame(mcrt_executor* ex, FrameParams fp, int total, int passes, ChunkCt
   const int cap = reserve_paths(ex, static_cast<long long>(total) * passes);
   const DScene scene = make_scene(ex);
   cuda_check(cudaEventRecord(ex->ev0, ex->stream), "cudaEventRecord");
-  for (int p0 = 0; p0 < total; p0 += cap) {
+  // This call's walk status alone, merged into the running stats afterwards.
+  const unsigned earlier = ex->stats.status;
+  ex->stats.status = 0;
+  cudaError_t e = cudaSuccess;
+  for (int p0 = 0; p0 < total && e == cudaSuccess; p0 += cap) {
     fp.pix0 = p0;
     fp.npix = std::min(cap, total - p0);
     ctx.fp = fp;
     Wavefront wf;
     wf.variant = ex->variant;
-    cuda_check(wf.run(scene, fp, passes, ex->paths, ex->stream, &ex->stats, ex->timed, chunk, &ctx), "render");
+    e = wf.run(scene, fp, passes, ex->paths, ex->stream, &ex->stats, ex->timed, chunk, &ctx);
   }
+  const unsigned walk = ex->stats.status;
+  ex->stats.status |= earlier;
+  cuda_check(e, "render");
   cuda_check(cudaEventRecord(ex->ev1, ex->stream), "cudaEventRecord");
   cuda_check(cudaEventSynchronize(ex->ev1), "render");
   float ms = 0;
   cudaEventElapsedTime(&ms, ex->ev0, ex->ev1);
   ex->ms_total += ms;
+  check_walk(walk);
 }
 
 void raytrace_impl(mcrt_executor* ex, int32_t gv, int32_t sv, const mcrt_camera* cam, const mcrt_settings* st,
@@ -901,6 +928,7 @@ int32_t mcrt_intersect_closest(mcrt_executor* ex, int32_t gv, int32_t count, con
     unsigned walk_status = 0;
     download(ex, &walk_status, fetch + 1, sizeof(unsigned), "download");
     ex->stats.status |= walk_status;
+    check_walk(walk_status);
     std::vector<int4> out(count);
     download(ex, out.data(), h, sizeof(int4) * count, "download");
     for (int i = 0; i < count; i++) {
@@ -920,8 +948,13 @@ int32_t mcrt_intersect_any_count(mcrt_executor* ex, int32_t gv, int32_t count, c
     if (count == 0) return;
     float4* r = static_cast<float4*>(ex->rays.upload(rays, sizeof(float) * 8 * count, ex->stream));
     int* c = static_cast<int*>(ex->hits.ensure(sizeof(int) * count));
-    unsigned* fetch = static_cast<unsigned*>(ex->scratch.ensure(sizeof(unsigned)));
+    unsigned* fetch = static_cast<unsigned*>(ex->scratch.ensure(2 * sizeof(unsigned)));
+    cuda_check(cudaMemsetAsync(fetch + 1, 0, sizeof(unsigned), ex->stream), "memset");
     cuda_check(launch_count_hits(make_scene(ex), r, count, c, fetch, ex->stream), "trace");
+    unsigned walk_status = 0;
+    download(ex, &walk_status, fetch + 1, sizeof(unsigned), "download");
+    ex->stats.status |= walk_status;
+    check_walk(walk_status);
     download(ex, counts, c, sizeof(int) * count, "download");
   });
 }
@@ -962,6 +995,7 @@ int32_t mcrt_intersect_closest_noalloc(mcrt_executor* ex, int32_t gv, int32_t co
     if (front) cuda_check(cudaMemcpyAsync(front, f_front, sizeof(int32_t) * count, d2h, s), "download");
     cuda_check(cudaStreamSynchronize(s), "download");
     ex->stats.status |= walk_status;
+    check_walk(walk_status);
   });
 }
 
@@ -1168,6 +1202,14 @@ int32_t mcrt_set_traversal(mcrt_executor* ex, int32_t block, int32_t stack) {
   });
 }
 
+int32_t mcrt_set_step_limit(mcrt_executor* ex, int32_t steps) {
+  return guard([&] {
+    checked(ex);
+    if (steps < 0) fail(MCRT_ERR_INVALID, "negative step limit");
+    ex->step_limit = steps;
+  });
+}
+
 int32_t mcrt_get_stats(mcrt_executor* ex, mcrt_stats* out) {
   return guard([&] {
     checked(ex);
@@ -1348,9 +1390,11 @@ int32_t mcrt_batch_step(mcrt_batch* b, mcrt_batch_event* events, int32_t max_eve
     check_slots(b);
     std::vector<BatchEvent> ev;
     bool is_idle = false;
+    const unsigned earlier = b->engine.totals().status;
     cuda_check(b->engine.step(ev, &is_idle), "batch step");
     if (b->engine.totals().status & kStatusIterationLimit)
       fail(MCRT_ERR_CUDA, "a batched chunk did not finish within its iteration limit");
+    check_walk(b->engine.totals().status & ~earlier);
     for (const BatchEvent& e : ev) b->pending.push_back(e);
     int n = 0;
     while (n < max_events && !b->pending.empty()) {
@@ -1375,9 +1419,11 @@ int32_t mcrt_batch_render(mcrt_batch* b, int32_t count, const mcrt_request* requ
       if (guard_steps > (1LL << 40)) fail(MCRT_ERR_LIMIT, "batch did not finish");
       check_slots(b);
       std::vector<BatchEvent> ev;
+      const unsigned earlier = b->engine.totals().status;
       cuda_check(b->engine.step(ev, &idle), "batch step");
       if (b->engine.totals().status & kStatusIterationLimit)
         fail(MCRT_ERR_CUDA, "a batched chunk did not finish within its iteration limit");
+      check_walk(b->engine.totals().status & ~earlier);
     }
   });
 }

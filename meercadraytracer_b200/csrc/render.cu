@@ -33,7 +33,10 @@ namespace cg = cooperative_groups;
 namespace mcrt {
 
 constexpr int kBlock = 128;
-constexpr int kShadowSeen = 16;  // de-duplicated see-through hits per shadow ray
+// De-duplicated see-through hits per shadow ray. The list is indexed at run
+// time, so it lives in local memory and costs nothing until a ray uses it; a
+// ray with more distinct see-through hits sets kStatusShadowListOverflow.
+constexpr int kShadowSeen = 64;
 constexpr int kSortMin = 1 << 16;  // shorter queues are shaded in the order they are in
 constexpr int kMaxIterations = 1 << 16;  // bounce / pass-through iterations of one chunk
 
@@ -1065,6 +1068,7 @@ __global__ void __launch_bounds__(kBlock) k_count_hits(DScene sc, const float4* 
   unsigned status = 0;
   CountQuery q{sc, rays, counts, 0, 0, 0.0f, {}};
   traverse_persistent(sc, q, n, fetch, st, status);
+  if (status) atomicOr(fetch + 1, status);
 }
 
 // ------------------------------------------------------------------- host

@@ -225,7 +225,8 @@ cudaError_t launch_batch_accumulate(const BatchTables* t, const PathState& ps, c
 cudaError_t launch_accumulate(const float4* samples, int npix, int passes_in_chunk, float4* sum, int total_passes,
                               int last_chunk, uint8_t* image, const FrameParams& fp, int srgb, cudaStream_t s);
 cudaError_t launch_tile_output(const float4* samples, const FrameParams& fp, float* out, cudaStream_t s);
-// `fetch` is a device counter the persistent traversal uses (reset here).
+// `fetch` is a device counter the persistent traversal uses (reset here);
+// fetch[1] collects the walk status bits (the caller clears it).
 cudaError_t launch_trace_rays(const DScene& scene, const float4* rays, int count, int cull, int4* hits,
                               unsigned* fetch, cudaStream_t s);
 cudaError_t launch_count_hits(const DScene& scene, const float4* rays, int count, int* counts, unsigned* fetch,

@@ -35,7 +35,7 @@
 
 namespace mcrt {
 
-constexpr int kShort = 16;  // default shared-memory stack entries per thread
+constexpr int kShort = 16;  // shared-memory stack entries per thread of the debugging kernels (k_trace_rays, k_count_hits)
 constexpr int kSentinel = 0x7fffffff;  // empty stack / finished ray
 constexpr int kLeafEnd = 1 << 16;      // in tris[3k].w: last triangle of its leaf
 constexpr int kRefill = 16;            // refill a warp's finished lanes once this many are idle
@@ -53,8 +53,8 @@ constexpr unsigned kStatusLeafRange = 8u;  // a leaf ran past the last triangle 
 // Node visits plus leaves one query may take: a walk of a well-formed BVH of
 // N triangles enters each of its fewer than 2N nodes at most once, so past
 // 2N + 64 steps something is wrong and the query ends (kStatusStepLimit)
-// instead of looping.
-MCRT_D int max_steps(const DScene& sc) { return 2 * sc.tri_count + 64; }
+// instead of looping. A positive sc.step_limit (a test hook) replaces it.
+MCRT_D int max_steps(const DScene& sc) { return sc.step_limit > 0 ? sc.step_limit : 2 * sc.tri_count + 64; }
 
 struct TravRay {
   V3 o, d, inv;

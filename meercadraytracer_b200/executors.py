@@ -440,6 +440,11 @@ class GpuExecutor:
         """Traversal kernels by threads per block and short-stack depth (_lib.traversal_variants())."""
         call("mcrt_set_traversal", self._h, int(block), int(stack))
 
+    def set_step_limit(self, steps: int) -> None:
+        """Test and debugging hook: node visits plus leaves one BVH query may take (0: the
+        default, 2N + 64 for N triangles); a query that runs out fails its call."""
+        call("mcrt_set_step_limit", self._h, int(steps))
+
     def stats(self) -> Dict[str, Any]:
         s = mcrt_stats()
         call("mcrt_get_stats", self._h, C.byref(s))

@@ -260,6 +260,7 @@ class DataTexture:
         self.flip_y = False
         self.color_space = NoColorSpace
         self.mapping = UVMapping
+        self.version = 0  # bump after editing the pixels in place (three.js texture.needsUpdate)
         self.id = DataTexture._next_id
         DataTexture._next_id += 1
 
@@ -271,6 +272,31 @@ class DataTexture:
         cx, cy = self.center
         return (sx * c, -sy * s, 0.0, sx * s, sy * c, 0.0,
                 -sx * (c * cx + s * cy) + cx + tx, -sy * (-s * cx + c * cy) + cy + ty, 1.0)
+
+
+class CubeTexture:
+    """Six RGBA face images (+x, -x, +y, -y, +z, -z), each first row first, as a
+    three.js CubeTexture holds them; mapping CubeReflectionMapping unless set."""
+
+    _next_id = 1
+
+    def __init__(self, images: Sequence[np.ndarray], width: int, height: int, format: int = RGBAFormat,
+                 type: Optional[int] = None):
+        if len(images) != 6:
+            raise ValueError("a cube texture has six face images")
+        self.images = [np.asarray(i) for i in images]
+        self.width, self.height, self.format = int(width), int(height), format
+        if type is None:
+            type = FloatType if self.images[0].dtype == np.float32 else UnsignedByteType
+        self.type = type
+        self.wrap_s = self.wrap_t = ClampToEdgeWrapping
+        self.flip_y = False
+        self.color_space = NoColorSpace
+        self.mapping = CubeReflectionMapping
+        self.is_render_target_texture = False
+        self.version = 0
+        self.id = CubeTexture._next_id
+        CubeTexture._next_id += 1
 
 
 # ------------------------------------------------------------------- geometry
@@ -414,6 +440,7 @@ class Material:
         self.normal_scale = (1.0, 1.0)
         self.ao_map_intensity = 1.0
         self.env_map_intensity: Optional[float] = None
+        self.env_map_rotation: Optional[Euler] = None
         self.reflectivity: Optional[float] = None
         self.combine: Optional[int] = None
         self._apply(kw)

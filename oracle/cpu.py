@@ -84,8 +84,11 @@ def lib() -> C.CDLL:
             getattr(L, name).argtypes = [d, d]
         L.oracle_sample_texture.argtypes = [P(abi.mcrt_texture), d, d, P(d)]
         L.oracle_sample_environment.argtypes = [P(abi.mcrt_environment), P(abi.mcrt_texture), d, d, d, P(d)]
+        L.oracle_plant_draw_mistake.argtypes = [i32]
         L.oracle_build_bvh.restype = i32
         L.oracle_build_bvh.argtypes = [P(C.c_float), i32, P(C.c_float), P(i32), P(u32)]
+        L.oracle_build_bvh_bins.restype = i32
+        L.oracle_build_bvh_bins.argtypes = [P(C.c_float), i32, i32, P(C.c_float), P(i32), P(u32)]
         L.oracle_intersect_closest.restype = i32
         L.oracle_intersect_closest.argtypes = [P(C.c_float), P(C.c_uint8), P(C.c_float), P(i32), i32, P(d), P(d),
                                                d, d, i32, P(oracle_hit), P(oracle_counters)]
@@ -96,7 +99,7 @@ def lib() -> C.CDLL:
         L.oracle_compile_geometry.argtypes = [
             i32, P(d), P(d), P(d), P(d), P(C.c_uint8), P(u32), P(C.c_uint8), P(C.c_uint8),
             P(C.c_float), P(C.c_float), P(C.c_float), P(C.c_float), P(C.c_float), P(u32), P(C.c_uint8),
-            P(C.c_uint8), P(C.c_float), P(i32), P(u32), P(i32), P(d), P(i32)]
+            P(C.c_uint8), P(C.c_float), P(i32), P(u32), P(i32), P(d), P(i32), i32]
         L.oracle_camera_ray.argtypes = [P(abi.mcrt_camera), d, d, P(d)]
         L.oracle_render_tile.restype = i32
         L.oracle_render_tile.argtypes = [P(abi.mcrt_geometry), P(abi.mcrt_shading), P(abi.mcrt_camera),
@@ -205,16 +208,22 @@ def sample_environment(env: CompiledEnvironment, textures: Sequence[CompiledText
     return list(out)
 
 
+def plant_draw_mistake(which: int) -> None:
+    """Test only: reorders one of the path loop's random draws in the oracle (1-6, see
+    oracle.cpp); 0 restores the reference's order."""
+    lib().oracle_plant_draw_mistake(int(which))
+
+
 # ------------------------------------------------------------------------ bvh
-def build_bvh(triangles: np.ndarray, count: int) -> Tuple[CompiledBvh, np.ndarray]:
-    """buildBvh, src/bvh.ts:16-178."""
+def build_bvh(triangles: np.ndarray, count: int, bins: int = 16) -> Tuple[CompiledBvh, np.ndarray]:
+    """buildBvh, src/bvh.ts:16-178, with `bins` SAH bins per axis (the reference's BINS is 16)."""
     tris = np.ascontiguousarray(triangles, np.float32)
     cap = max(1, 2 * count - 1)
     bounds = np.zeros(cap * 6, np.float32)
     nodes = np.zeros(cap * 3, np.int32)
     order = np.zeros(max(1, count), np.uint32)
-    n = lib().oracle_build_bvh(_p(tris, C.c_float), count, _p(bounds, C.c_float), _p(nodes, C.c_int32),
-                               _p(order, C.c_uint32))
+    n = lib().oracle_build_bvh_bins(_p(tris, C.c_float), count, int(bins), _p(bounds, C.c_float),
+                                    _p(nodes, C.c_int32), _p(order, C.c_uint32))
     return CompiledBvh(bounds[: n * 6].copy(), nodes[: n * 3].copy(), int(n)), order[:count].copy()
 
 
@@ -240,8 +249,9 @@ def intersect_any_count(triangles: np.ndarray, bvh: CompiledBvh, o: Sequence[flo
 
 
 # -------------------------------------------------------------------- compile
-def compile_sink(sink: TriangleSink) -> CompiledGeometry:
-    """compileGeometry after the flatten (src/compile.ts:359-403): the oracle's geometry builder."""
+def compile_sink(sink: TriangleSink, bins: int = 16) -> CompiledGeometry:
+    """compileGeometry after the flatten (src/compile.ts:359-403): the oracle's geometry builder,
+    with `bins` SAH bins per axis in the BVH build (16 as the reference)."""
     n = sink.count
     cap = max(1, 2 * n - 1)
     f32, u8, u32 = np.float32, np.uint8, np.uint32
@@ -260,7 +270,7 @@ def compile_sink(sink: TriangleSink) -> CompiledGeometry:
         _p(ss, C.c_uint8), _p(tris, C.c_float), _p(nrm, C.c_float), _p(uvs, C.c_float), _p(tan, C.c_float),
         _p(colors, C.c_float), _p(mats, C.c_uint32), _p(flags, C.c_uint8), _p(sides, C.c_uint8),
         _p(bounds, C.c_float), _p(nodes, C.c_int32), _p(order, C.c_uint32), C.byref(node_count), C.byref(eps),
-        C.byref(any_colors))
+        C.byref(any_colors), int(bins))
     m = int(node_count.value)
     return CompiledGeometry(
         triangle_count=n, triangles=tris, normals=nrm, uvs=uvs, tangents=tan,

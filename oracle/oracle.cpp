@@ -91,6 +91,18 @@ struct Random {
   }
 };
 
+// A mistake planted in the path loop's use of random numbers, for tests that
+// show a comparison would catch a reordered, extra or missing draw. 0 (the
+// default) is the reference's order. Set only by oracle_plant_draw_mistake.
+//   1  the transparency test (tracer.ts:170) draws twice
+//   2  the GI-off environment estimate's cosine draws (tracer.ts:343-344,
+//      601) are taken in swapped order
+//   3  the continuation pick (tracer.ts:420) draws twice
+//   4  the diffuse continuation's cosine draws (tracer.ts:455, 601) swapped
+//   5  the GGX half-vector draws (tracer.ts:610-612) swapped
+//   6  Russian roulette (tracer.ts:465-467) draws from bounce 2 on, not 3
+int g_planted_draw_mistake = 0;
+
 // ----------------------------------------------------------------- color.ts
 
 double srgb_to_linear(double c) {  // color.ts:11-13
@@ -391,7 +403,8 @@ void sample_environment(const mcrt_environment& env, const mcrt_texture* texture
 
 // ------------------------------------------------------------------- bvh.ts
 
-const int kBins = 16;      // bvh.ts:3
+const int kBins = 16;      // bvh.ts:3 (BINS); build_bvh takes the count as a parameter
+const int kMaxBins = 64;
 const int kMaxLeaf = 4;    // bvh.ts:4
 const int kMaxDepth = 100; // bvh.ts:5
 
@@ -400,9 +413,14 @@ double area(double x0, double y0, double z0, double x1, double y1, double z1) { 
   return dx * dy + dy * dz + dz * dx;
 }
 
-// buildBvh, bvh.ts:16-178. Returns nodeCount.
-int32_t build_bvh(const float* tris, int32_t count, float* bounds, int32_t* nodes, uint32_t* order) {
+// buildBvh, bvh.ts:16-178, with BINS (bvh.ts:3) as the parameter `bins`: the
+// reference's builder is written in terms of that one constant, so a build
+// with another bin count is the same algorithm. Returns nodeCount.
+int32_t build_bvh(const float* tris, int32_t count, float* bounds, int32_t* nodes, uint32_t* order,
+                  int bins = kBins) {
   if (count == 0) return 0;
+  if (bins < 2) bins = 2;
+  if (bins > kMaxBins) bins = kMaxBins;
   std::vector<float> cent[3];
   for (auto& c : cent) c.resize(count);
   std::vector<float> bmin(static_cast<size_t>(count) * 3), bmax(static_cast<size_t>(count) * 3);
@@ -424,10 +442,10 @@ int32_t build_bvh(const float* tris, int32_t count, float* bounds, int32_t* node
   struct Item { int32_t node, first, n, depth; };
   std::vector<Item> stack;
   stack.push_back({0, 0, count, 0});
-  int32_t bin_count[kBins];
-  float bin_bounds[kBins * 6];
-  double right_area[kBins];
-  int32_t right_count[kBins];
+  int32_t bin_count[kMaxBins];
+  float bin_bounds[kMaxBins * 6];
+  double right_area[kMaxBins];
+  int32_t right_count[kMaxBins];
   while (!stack.empty()) {
     Item it = stack.back();
     stack.pop_back();
@@ -466,17 +484,17 @@ int32_t build_bvh(const float* tris, int32_t count, float* bounds, int32_t* node
     for (int axis = 0; axis < 3; axis++) {
       double lo = cmin[axis], extent = cmax[axis] - lo;
       if (!(extent > 0)) continue;
-      double scale = kBins / extent;
+      double scale = bins / extent;
       const std::vector<float>& c = cent[axis];
-      std::fill(bin_count, bin_count + kBins, 0);
-      for (int i = 0; i < kBins; i++) {
+      std::fill(bin_count, bin_count + bins, 0);
+      for (int i = 0; i < bins; i++) {
         float* o = bin_bounds + i * 6;
         o[0] = o[1] = o[2] = std::numeric_limits<float>::infinity();
         o[3] = o[4] = o[5] = -std::numeric_limits<float>::infinity();
       }
       for (int32_t k = first; k < first + n; k++) {
         uint32_t t = order[k];
-        int bin = static_cast<int>(std::min(static_cast<double>(kBins - 1), std::floor((c[t] - lo) * scale)));
+        int bin = static_cast<int>(std::min(static_cast<double>(bins - 1), std::floor((c[t] - lo) * scale)));
         bin_count[bin]++;
         float* o = bin_bounds + bin * 6;
         for (int a = 0; a < 3; a++) {
@@ -486,7 +504,7 @@ int32_t build_bvh(const float* tris, int32_t count, float* bounds, int32_t* node
       }
       double rx0 = kInf, ry0 = kInf, rz0 = kInf, rx1 = -kInf, ry1 = -kInf, rz1 = -kInf;
       int32_t rc = 0;
-      for (int i = kBins - 1; i > 0; i--) {
+      for (int i = bins - 1; i > 0; i--) {
         const float* o = bin_bounds + i * 6;
         rc += bin_count[i];
         rx0 = std::min(rx0, static_cast<double>(o[0])); ry0 = std::min(ry0, static_cast<double>(o[1]));
@@ -498,7 +516,7 @@ int32_t build_bvh(const float* tris, int32_t count, float* bounds, int32_t* node
       }
       double lx0 = kInf, ly0 = kInf, lz0 = kInf, lx1 = -kInf, ly1 = -kInf, lz1 = -kInf;
       int32_t lc = 0;
-      for (int i = 0; i < kBins - 1; i++) {
+      for (int i = 0; i < bins - 1; i++) {
         const float* o = bin_bounds + i * 6;
         lc += bin_count[i];
         lx0 = std::min(lx0, static_cast<double>(o[0])); ly0 = std::min(ly0, static_cast<double>(o[1]));
@@ -523,11 +541,11 @@ int32_t build_bvh(const float* tris, int32_t count, float* bounds, int32_t* node
         nd[0] = first; nd[1] = n; nd[2] = 0;
         continue;
       }
-      double lo = cmin[best_axis], scale = kBins / (cmax[best_axis] - lo);
+      double lo = cmin[best_axis], scale = bins / (cmax[best_axis] - lo);
       const std::vector<float>& c = cent[best_axis];
       int32_t i = first, j = first + n - 1;
       while (i <= j) {
-        int bin = static_cast<int>(std::min(static_cast<double>(kBins - 1), std::floor((c[order[i]] - lo) * scale)));
+        int bin = static_cast<int>(std::min(static_cast<double>(bins - 1), std::floor((c[order[i]] - lo) * scale)));
         if (bin <= best_split) {
           i++;
         } else {
@@ -869,7 +887,8 @@ struct Tracer {
         alpha *= texel[1];
       }
       bool cut_out = mat.alpha_test > 0 && alpha < mat.alpha_test;
-      if (cut_out || (mat.transparent && random.next() >= alpha)) {
+      if (cut_out || (mat.transparent && (g_planted_draw_mistake == 1 ? (random.next(), random.next())
+                                                                       : random.next()) >= alpha)) {
         if (++passes > kMaxPassThrough) break;
         double side = gx * dx + gy * dy + gz * dz > 0 ? eps : -eps;
         ox = px + gx * side; oy = py + gy * side; oz = pz + gz * side;
@@ -1037,7 +1056,7 @@ struct Tracer {
             environment_scale = mat.env_map_intensity;
           }
           if (environment && !settings.global_illumination) {
-            cosine_direction(nx, ny, nz);
+            cosine_direction(nx, ny, nz, g_planted_draw_mistake == 2);
             const double sx2 = sx, sy2 = sy, sz2 = sz;
             if (sx2 * gx + sy2 * gy + sz2 * gz > 0 &&
                 transmittance(px + gx * eps, py + gy * eps, pz + gz * eps, sx2, sy2, sz2, kInf, false)) {
@@ -1114,6 +1133,7 @@ struct Tracer {
       const double wd = luminance(diff_r, diff_g, diff_b);
       const double total = ws + wt + wd;
       if (total <= 1e-6) break;
+      if (g_planted_draw_mistake == 3) random.next();
       const double pick = random.next() * total;
       double wr, wg, wb, p;
       if (pick < ws) {
@@ -1146,7 +1166,7 @@ struct Tracer {
       } else {
         p = wd / total;
         wr = diff_r; wg = diff_g; wb = diff_b;
-        cosine_direction(nx, ny, nz);
+        cosine_direction(nx, ny, nz, g_planted_draw_mistake == 4);
         if (sx * gx + sy * gy + sz * gz <= 0) break;
         last_env = environment;
         last_env_scale = environment_scale;
@@ -1156,7 +1176,7 @@ struct Tracer {
       ox = px + gx * side; oy = py + gy * side; oz = pz + gz * side;
       dx = sx; dy = sy; dz = sz;
       bounce++;
-      if (bounce >= 3) {
+      if (bounce >= (g_planted_draw_mistake == 6 ? 2 : 3)) {
         const double q = std::min(0.95, std::max(tr, std::max(tg, tb)));
         if (random.next() >= q) break;
         tr /= q; tg /= q; tb /= q;
@@ -1286,8 +1306,9 @@ struct Tracer {
   }
 
   // cosineDirection, tracer.ts:600-605.
-  void cosine_direction(double nx, double ny, double nz) {
-    const double r1 = random.next(), r2 = random.next();
+  void cosine_direction(double nx, double ny, double nz, bool swapped = false) {
+    double r1 = random.next(), r2 = random.next();
+    if (swapped) std::swap(r1, r2);
     const double phi = 2 * kPi * r1;
     const double radius = std::sqrt(r2);
     to_world(nx, ny, nz, radius * std::cos(phi), radius * std::sin(phi), std::sqrt(std::max(0.0, 1 - r2)));
@@ -1298,7 +1319,8 @@ struct Tracer {
     double hx = nx, hy = ny, hz = nz;
     if (roughness > 0.02) {
       const double a = roughness * roughness;
-      const double r1 = random.next(), r2 = random.next();
+      double r1 = random.next(), r2 = random.next();
+      if (g_planted_draw_mistake == 5) std::swap(r1, r2);
       const double phi = 2 * kPi * r1;
       const double cos_theta = std::sqrt((1 - r2) / (1 + (a * a - 1) * r2));
       const double sin_theta = std::sqrt(std::max(0.0, 1 - cos_theta * cos_theta));
@@ -1454,6 +1476,8 @@ extern "C" {
 
 uint32_t oracle_hash(uint32_t x) { return hash32(x); }
 
+void oracle_plant_draw_mistake(int32_t which) { g_planted_draw_mistake = which; }
+
 uint32_t oracle_seed(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
   Random r;
   r.seed(a, b, c, d);
@@ -1495,6 +1519,11 @@ int32_t oracle_build_bvh(const float* triangles, int32_t count, float* bounds, i
   return build_bvh(triangles, count, bounds, nodes, order);
 }
 
+int32_t oracle_build_bvh_bins(const float* triangles, int32_t count, int32_t bins, float* bounds, int32_t* nodes,
+                              uint32_t* order) {
+  return build_bvh(triangles, count, bounds, nodes, order, bins);
+}
+
 int32_t oracle_intersect_closest(const float* triangles, const uint8_t* sides, const float* bounds,
                                  const int32_t* nodes, int32_t node_count, const double* o, const double* d,
                                  double t_min, double t_max, int32_t cull, oracle_hit* out,
@@ -1533,7 +1562,8 @@ int32_t oracle_compile_geometry(int32_t count, const double* p, const double* n,
                                 float* normals_out, float* uvs_out, float* tangents_out, float* colors_out,
                                 uint32_t* materials_out, uint8_t* flags_out, uint8_t* sides_out,
                                 float* bounds_out, int32_t* nodes_out, uint32_t* order_out,
-                                int32_t* node_count_out, double* epsilon_out, int32_t* any_colors) {
+                                int32_t* node_count_out, double* epsilon_out, int32_t* any_colors,
+                                int32_t bins) {
   std::vector<float> tris(static_cast<size_t>(count) * 9);
   double max_coordinate = 0;
   bool any = false;
@@ -1549,7 +1579,7 @@ int32_t oracle_compile_geometry(int32_t count, const double* p, const double* n,
     if (has_color && has_color[i]) any = true;
   }
   *any_colors = any ? 1 : 0;
-  int32_t node_count = build_bvh(tris.data(), count, bounds_out, nodes_out, order_out);
+  int32_t node_count = build_bvh(tris.data(), count, bounds_out, nodes_out, order_out, bins > 0 ? bins : kBins);
   *node_count_out = node_count;
   double min_x = kInf, min_y = kInf, min_z = kInf, max_x = -kInf, max_y = -kInf, max_z = -kInf;
   for (int32_t i = 0; i < count; i++) {

@@ -69,9 +69,17 @@ void oracle_sample_texture(const mcrt_texture* texture, double u, double v, doub
 void oracle_sample_environment(const mcrt_environment* env, const mcrt_texture* textures,
                                double dx, double dy, double dz, double* out3);
 
+/* Test only: plants mistake `which` (1-6, see oracle.cpp) in the order the
+ * path loop draws random numbers; 0 restores the reference's order. Process
+ * wide: set it only while no render runs. */
+void oracle_plant_draw_mistake(int32_t which);
+
 /* bvh.ts. Output arrays hold max(1, 2 * count - 1) nodes; returns nodeCount. */
 int32_t oracle_build_bvh(const float* triangles, int32_t count, float* bounds, int32_t* nodes,
                          uint32_t* order);
+/* The same build with `bins` bins per axis (bvh.ts:3's BINS; 2 to 64). */
+int32_t oracle_build_bvh_bins(const float* triangles, int32_t count, int32_t bins, float* bounds,
+                              int32_t* nodes, uint32_t* order);
 int32_t oracle_intersect_closest(const float* triangles, const uint8_t* sides, const float* bounds,
                                  const int32_t* nodes, int32_t node_count, const double* origin,
                                  const double* direction, double t_min, double t_max, int32_t cull,
@@ -88,6 +96,7 @@ int32_t oracle_intersect_any_count(const float* triangles, const float* bounds, 
  * has_color[k] saying whether triangle k carried vertex colours.
  * Outputs are sized for `count` triangles and max(1, 2 count - 1) nodes;
  * colors_out is written only if any triangle has colours (returned in *any_colors).
+ * `bins`: SAH bins per axis of the BVH build (16 as the reference; 0 means 16).
  */
 int32_t oracle_compile_geometry(int32_t count, const double* p, const double* n, const double* uv,
                                 const double* colors, const uint8_t* has_color,
@@ -96,7 +105,7 @@ int32_t oracle_compile_geometry(int32_t count, const double* p, const double* n,
                                 float* tangents_out, float* colors_out, uint32_t* materials_out,
                                 uint8_t* flags_out, uint8_t* sides_out, float* bounds_out,
                                 int32_t* nodes_out, uint32_t* order_out, int32_t* node_count_out,
-                                double* epsilon_out, int32_t* any_colors);
+                                double* epsilon_out, int32_t* any_colors, int32_t bins);
 
 /* tracer.ts cameraRay (src/tracer.ts:705-727): origin then direction. */
 void oracle_camera_ray(const mcrt_camera* camera, double x, double y, double* out6);

@@ -9,6 +9,9 @@ to render a whole frame.
     and the batch engine's image of it is within one level of the plain path's.
   * Instanced geometry at 4,096,000 triangles (200 icospheres subdivided 5 times): the device
     flatten + compile equals the GPU compile of the host flatten, arrays and tree.
+  * The per-frame rebuild workload's build (32 bins, leaves of 4) on a 4,096,000-triangle frame:
+    the device tree equals the oracle's 32-bin tree of the same triangles, and camera rays of the
+    2048 x 2048 frame hit what the oracle's hit on a 16,384-pixel sample.
 """
 import numpy as np
 import pytest
@@ -105,6 +108,58 @@ def test_mid_frame_is_deterministic_and_batched_within_one_level(mid):
         assert d.max() <= 1 and (d.reshape(-1, 4).max(axis=1) > 0).mean() < 1e-4
     finally:
         r.dispose()
+
+
+def _large_frame_sink(big, instances):
+    from meercadraytracer_b200.compile import TriangleSink
+
+    parts = []
+    for world, mesh, material, flags, side, flat in instances:
+        m = S.Mesh(big.mesh, S.MeshStandardMaterial())
+        m.cast_shadow = m.receive_shadow = True
+        m.matrix_world = np.asarray(world, np.float64)
+        parts.append(flatten_meshes([m], lambda _m, k=material: k))
+    cat = lambda name: np.concatenate([getattr(p, name) for p in parts])  # noqa: E731
+    return TriangleSink(cat("p"), cat("n"), cat("uv"), cat("colors"), cat("has_color"), cat("materials"),
+                        cat("flags"), cat("sides"))
+
+
+def test_rebuild_frame_with_32_bins_equals_oracle_tree_and_hits():
+    from meercadraytracer_b200.executors import GpuExecutor
+
+    big = scenes.large_scene(count=200)
+    instances = big.frame(1)
+    sink = _large_frame_sink(big, instances)
+    assert sink.count == 200 * 20480
+    o = cpu.compile_sink(sink, bins=32)
+    ex = GpuExecutor(0)
+    try:
+        ex.upload_meshes([big.mesh])
+        info, dev = ex.compile_instances(instances, bins=32, download=True)
+        assert info["bins"] == 32 and dev.bvh.node_count == o.bvh.node_count
+        assert canonical(dev.bvh, dev.order) == canonical(o.bvh, o.order)
+        inv_o, inv_d = np.argsort(o.order), np.argsort(dev.order)
+        assert np.array_equal(o.triangles.reshape(-1, 9)[inv_o], dev.triangles.reshape(-1, 9)[inv_d])
+        cam = compile_camera(big.camera)
+        rng = np.random.default_rng(9)
+        idx = rng.choice(big.width * big.height, 16384, replace=False)
+        px, py = (idx % big.width).astype(np.int32), (idx // big.width).astype(np.int32)
+        scene_d = CompiledScene(dev, big.compiled.materials, big.compiled.textures, [], big.compiled.lights,
+                                big.compiled.background, -1, None)
+        scene_o = CompiledScene(o, big.compiled.materials, big.compiled.textures, [], big.compiled.lights,
+                                big.compiled.background, -1, None)
+        g = ex.trace_primary(scene_d, cam, big.width, big.height, 2, 0, px, py)
+        r = cpu.trace_primary(scene_o, cam, big.width, big.height, 2, 0, px, py, threads=8)
+        g_in = np.where(g["tri"] >= 0, dev.order[np.maximum(g["tri"], 0)], -1)
+        r_in = np.where(r["tri"] >= 0, o.order[np.maximum(r["tri"], 0)], -1)
+        same = g_in == r_in
+        hit = r_in >= 0
+        ties = ~same & (g_in >= 0) & hit & (np.abs(g["t"] - r["t"]) <= 1e-5 * np.abs(r["t"]))
+        assert same.mean() >= 0.9999 or (~same == ties).all(), (same.mean(), int((~same).sum()), int(ties.sum()))
+        rel = np.abs(g["t"][hit & same] - r["t"][hit & same]) / r["t"][hit & same]
+        assert hit.sum() > 1000 and rel.max() <= 1e-5
+    finally:
+        ex.dispose()
 
 
 def test_instanced_compile_at_four_million_triangles_equals_host_flatten():

@@ -10,9 +10,11 @@ use the same seed on both sides, as the reference's own determinism tests
 do (tests/render.test.ts:321-327).
 
 Scenes: the small scene with GI turned on (ground bounce, metal and rough
-spheres, directional + point light), and a reduced mid scene (6 x 6
-displaced icospheres, Standard / transmissive Physical / Phong materials,
-noise albedo maps, 4 point lights + hemisphere light), camera moved in.
+spheres, directional + point light), a reduced mid scene (6 x 6 displaced
+icospheres, Standard / transmissive Physical / Phong materials, noise albedo
+maps, 4 point lights + hemisphere light), camera moved in, and the mid scene
+itself at its benchmarked size (1,310,720 triangles, 1920 x 1080, GI on,
+4 bounces, ACES, sRGB) on 1024 seeded pixels whose camera ray hits geometry.
 """
 import os
 
@@ -55,14 +57,24 @@ def _mid_reduced():
     return b
 
 
-@pytest.fixture(scope="module", params=["small_gi", "mid_reduced"])
+@pytest.fixture(scope="module", params=["small_gi", "mid_reduced", "mid_full"])
 def case(request):
-    b = _small() if request.param == "small_gi" else _mid_reduced()
+    b = {"small_gi": _small, "mid_reduced": _mid_reduced, "mid_full": scenes.mid_scene}[request.param]()
     compiled = compile_scene(b.scene, builder=cpu.compile_sink)
     cam = compile_camera(b.camera)
     rng = np.random.default_rng(11)
-    idx = rng.choice(b.width * b.height, PIXELS, replace=False)
-    px, py = (idx % b.width).astype(np.int32), (idx // b.width).astype(np.int32)
+    if request.param == "mid_full":
+        # Three quarters of the 1080p frame is background: keep pixels whose
+        # pass-0 camera ray hits a triangle.
+        idx = rng.choice(b.width * b.height, 16 * PIXELS, replace=False)
+        px, py = (idx % b.width).astype(np.int32), (idx // b.width).astype(np.int32)
+        hit = cpu.trace_primary(compiled, cam, b.width, b.height, 0, 0, px, py, threads=THREADS)["tri"] >= 0
+        keep = np.nonzero(hit)[0][:PIXELS]
+        assert keep.size == PIXELS
+        px, py = px[keep], py[keep]
+    else:
+        idx = rng.choice(b.width * b.height, PIXELS, replace=False)
+        px, py = (idx % b.width).astype(np.int32), (idx // b.width).astype(np.int32)
     st_ref = trace_settings(as_options(b.options, seed=REFERENCE_SEED))
     _, sums = cpu.render_pixels(compiled, cam, st_ref, b.width, b.height, REFERENCE_SPP, True, px, py,
                                 threads=THREADS)

@@ -116,6 +116,28 @@ def test_closest_and_all_hits_match_brute_force(bvh3000):  # bvh.test.ts:82-107
     assert hits > 100
 
 
+@pytest.mark.parametrize("bins", [16, 32])
+def test_bin_count_parameter(bvh3000, bins):
+    """BINS (bvh.ts:3) as a parameter: 16 is the default build, and a 32-bin tree of the
+    same triangles is another valid BVH (every triangle once, hits equal brute force)
+    whose split decisions differ."""
+    raw, bvh16, order16, _ = bvh3000
+    bvh, order = cpu.build_bvh(raw, 3000, bins=bins)
+    assert sorted(order.tolist()) == list(range(3000))
+    if bins == 16:
+        assert np.array_equal(bvh.nodes, bvh16.nodes) and np.array_equal(order, order16)
+        return
+    assert not (bvh.node_count == bvh16.node_count and np.array_equal(order, order16))
+    data = reorder(raw, order)
+    sides = np.full(3000, 2, np.uint8)
+    for i in range(0, 400, 4):
+        o, d = lissajous_ray(i)
+        best, tri, allhits = brute_force(data, o, d)
+        found, hit = cpu.intersect_closest(data, sides, bvh, o, d)
+        assert found == (tri >= 0) and (not found or hit.triangle == tri)
+        assert cpu.intersect_any_count(data, bvh, o, d) == allhits
+
+
 def test_culling_front_back_double():  # bvh.test.ts:109-123
     tri = np.array([-1, -1, 0, 2, 0, 0, 0, 2, 0], np.float32)
     bvh, _ = cpu.build_bvh(tri, 1)
