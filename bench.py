@@ -369,13 +369,6 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                             "peak_source": peaks["source"], "traffic": traffic_from_profile(top),
                             "bytes_per_query": round(bpq["closest" if top == "extend" else "any"], 1),
                             "algorithmic_bytes_per_launch": round(per_launch_bytes)}
-        # The scene's nodes and triangles (~100 MB) fit the 126 MB L2, so the same bytes
-        # against the L2's own copy bandwidth, measured here, are the tighter roof.
-        l2 = measure_l2_gbs(local)
-        line["roofline_l2"] = {"bound": "l2", "kernel": f"k_{top}", "achieved": round(achieved, 1),
-                               "peak": round(l2, 1), "unit": "GB/s", "frac": round(achieved / l2, 4),
-                               "peak_source": "measured in this run: 16 MiB device-to-device copies, "
-                                              "read + write bytes, best of 5 rounds of 200"}
         line["cpu_baseline"] = {"value": round(base["mrays_s"], 3), "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{base['pixels']} random pixels x {spp} passes ({base['rays']} rays, "
                                           f"{base['seconds']:.1f} s) of the same workload on the oracle, a C++ "
@@ -625,27 +618,6 @@ def run_large(device: int, count: int, frames: int, bins: int = 32, tune: bool =
         return out
     finally:
         ex.dispose()
-
-
-def measure_l2_gbs(device: int) -> float:
-    """Copy bandwidth of a 16 MiB to 16 MiB device copy (32 MiB in flight, well inside
-    the 126 MB L2), read + write bytes per second, best of 5 rounds of 200 copies."""
-    import torch
-
-    x = torch.ones(16 << 20, dtype=torch.uint8, device=f"cuda:{device}")
-    y = torch.empty_like(x)
-    for _ in range(20):
-        y.copy_(x)
-    best = 0.0
-    for _ in range(5):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        for _ in range(200):
-            y.copy_(x)
-        b.record()
-        b.synchronize()
-        best = max(best, 2 * x.numel() * 200 / (a.elapsed_time(b) / 1e3) / 1e9)
-    return best
 
 
 def traffic_from_profile(kernel: str) -> Optional[float]:

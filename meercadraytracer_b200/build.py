@@ -27,9 +27,11 @@ SOURCES = {
     "render.cu": [],
     "executor.cu": [],
     "batch.cu": [],
+    "wide_bvh.cu": [],
     "scene_build.cu": ["--fmad=false"],
 }
-HEADERS = ["mcrt_math.cuh", "device_scene.cuh", "traverse.cuh", "render.cuh", "scene_build.cuh", "batch.cuh", "dfg_lut.h"]
+HEADERS = ["mcrt_math.cuh", "device_scene.cuh", "traverse.cuh", "render.cuh", "scene_build.cuh", "batch.cuh", "dfg_lut.h",
+           "wide_bvh.cuh"]
 
 
 def nvcc() -> str:

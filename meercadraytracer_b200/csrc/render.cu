@@ -49,6 +49,37 @@ MCRT_D unsigned int queue_append(unsigned int* counter) {
   return base + g.thread_rank();
 }
 
+// ------------------------------------------------------------------- walks
+// The traversal every query kernel runs: the compressed 8-wide BVH, or the
+// binary tree when built with MCRT_BINARY_WALK. B threads per block, S
+// shared-memory stack entries per thread, warps refilled once REFILL lanes
+// are idle.
+#ifdef MCRT_BINARY_WALK
+constexpr bool kWideWalk = false;
+#else
+constexpr bool kWideWalk = true;
+#endif
+constexpr int kPostpone = 8;  // wide walk: triangle tests postponed while fewer lanes than this test triangles
+
+template <int REFILL, int B, int S, class Q>
+MCRT_D void walk(const DScene& sc, Q& q, int n, unsigned* counter, unsigned& status) {
+  if constexpr (kWideWalk) {
+    __shared__ uint2 wide_stack[S * B];
+    WideStackT<S> st;
+    st.smem = wide_stack + threadIdx.x;
+    st.stride = B;
+    st.sp = 0;
+    traverse_wide<REFILL, kPostpone>(sc, q, n, counter, st, status);
+  } else {
+    __shared__ int binary_stack[S * B];
+    TravStackT<S> st;
+    st.smem = binary_stack + threadIdx.x;
+    st.stride = B;
+    st.sp = 0;
+    traverse_persistent<REFILL>(sc, q, n, counter, st, status);
+  }
+}
+
 // ---------------------------------------------------------------- mapping
 MCRT_D void path_pixel(const FrameParams& fp, int pid, int& px, int& py, int& pass) {
   const int k = pid - fp.path_base;
@@ -142,6 +173,7 @@ struct ExtendQuery {
   MCRT_D const TravRay& ray() const { return cs.r; }
   MCRT_D float t_max() const { return cs.tmax; }
   MCRT_D bool leaf(int first) { return cs.leaf(sc, first); }
+  MCRT_D bool tri(int k) { return cs.wide_tri(sc, k); }
   MCRT_D void finish() {
     const ClosestHit& h = cs.h;
     const unsigned word = h.tri >= 0 ? ((h.front ? 0x80000000u : 0u) | static_cast<unsigned>(h.tri + 1)) : 0u;
@@ -150,19 +182,16 @@ struct ExtendQuery {
 };
 
 // B threads per block, S short-stack entries per thread (a traversal variant).
-// 1280 / B blocks per SM: the register cap (48) costs a few bytes of spills
-// and buys a ninth more resident warps than the unconstrained 56 registers.
+// kExtendBlocks128 blocks of 128 threads per SM set the register cap: the
+// binary walk at 10 (48 registers, a few bytes of spills, a ninth more
+// resident warps than its unconstrained 56); the wide walk at 9 (56).
+constexpr int kExtendBlocks128 = kWideWalk ? 9 : 10;
 template <int B, int S>
-__global__ void __launch_bounds__(B, 1280 / B) k_extend(DScene sc, PathState ps, const int* __restrict__ queue, int n,
+__global__ void __launch_bounds__(B, kExtendBlocks128 * 128 / B) k_extend(DScene sc, PathState ps, const int* __restrict__ queue, int n,
                                               Counters* cnt) {
-  __shared__ int stack_mem[S * B];
-  TravStackT<S> st;
-  st.smem = stack_mem + threadIdx.x;
-  st.stride = B;
-  st.sp = 0;
   unsigned status = 0;
   ExtendQuery q{sc, ps, queue, 0, {}};
-  traverse_persistent<kRefillClosest>(sc, q, n, &cnt->fetch, st, status);
+  walk<kRefillClosest, B, S>(sc, q, n, &cnt->fetch, status);
   if (status) atomicOr(&cnt->status, status);
 }
 
@@ -811,6 +840,14 @@ struct ShadowQuery {
     }
     return true;
   }
+  // Wide-order triangle k; false once the ray is blocked.
+  MCRT_D bool tri(int k) {
+    const float4* p = sc.wtris + 3 * static_cast<size_t>(k);
+    const float4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2);
+    TriHit th;
+    return !(intersect_triangle(r, V3{w0.x, w0.y, w0.z}, V3{w1.x, w1.y, w1.z}, V3{w2.x, w2.y, w2.z}, max_t, 2, th) &&
+             visit(__float_as_int(w2.w), th, w0, w1));
+  }
   // One hit of the visitor; true once the ray is blocked.
   MCRT_D bool visit(int k, const TriHit& th, float4 w0, float4 w1) {
     const int fl = tri_flags(w0.w);
@@ -876,14 +913,9 @@ struct ShadowQuery {
 // of 48 spills in the walk itself and measured 40 % slower.
 template <int B, int S>
 __global__ void __launch_bounds__(B, 1152 / B) k_shadow(DScene sc, PathState ps, int n, int capacity, Counters* cnt) {
-  __shared__ int stack_mem[S * B];
-  TravStackT<S> st;
-  st.smem = stack_mem + threadIdx.x;
-  st.stride = B;
-  st.sp = 0;
   unsigned status = 0;
   ShadowQuery q{sc, ps, capacity, &status};
-  traverse_persistent<kRefillShadow>(sc, q, n, &cnt->fetch_shadow, st, status);
+  walk<kRefillShadow, B, S>(sc, q, n, &cnt->fetch_shadow, status);
   if (status) atomicOr(&cnt->status, status);
 }
 
@@ -1008,6 +1040,7 @@ struct RayQuery {
   MCRT_D const TravRay& ray() const { return cs.r; }
   MCRT_D float t_max() const { return cs.tmax; }
   MCRT_D bool leaf(int first) { return cs.leaf(sc, first); }
+  MCRT_D bool tri(int k) { return cs.wide_tri(sc, k); }
   MCRT_D void finish() {
     hits[i] = make_int4(cs.h.tri, __float_as_int(cs.h.t), __float_as_int(cs.h.u),
                         (cs.h.front ? 1 : 0) | (min(cs.tests, 0xffffff) << 8));
@@ -1016,14 +1049,9 @@ struct RayQuery {
 
 __global__ void __launch_bounds__(kBlock) k_trace_rays(DScene sc, const float4* __restrict__ rays, int n, int cull,
                                                        int4* __restrict__ hits, unsigned* fetch) {
-  __shared__ int stack_mem[kShort * kBlock];
-  TravStack st;
-  st.smem = stack_mem + threadIdx.x;
-  st.stride = kBlock;
-  st.sp = 0;
   unsigned status = 0;
   RayQuery q{sc, rays, cull, hits, 0, {}};
-  traverse_persistent(sc, q, n, fetch, st, status);
+  walk<kRefill, kBlock, kShort>(sc, q, n, fetch, status);
   if (status) atomicOr(fetch + 1, status);
 }
 
@@ -1055,19 +1083,21 @@ struct CountQuery {
     }
     return true;
   }
+  MCRT_D bool tri(int k) {
+    const float4* p = sc.wtris + 3 * static_cast<size_t>(k);
+    const float4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2);
+    TriHit th;
+    if (intersect_triangle(r, V3{w0.x, w0.y, w0.z}, V3{w1.x, w1.y, w1.z}, V3{w2.x, w2.y, w2.z}, limit, 2, th)) hits++;
+    return true;
+  }
   MCRT_D void finish() { counts[i] = hits; }
 };
 
 __global__ void __launch_bounds__(kBlock) k_count_hits(DScene sc, const float4* __restrict__ rays, int n,
                                                        int* __restrict__ counts, unsigned* fetch) {
-  __shared__ int stack_mem[kShort * kBlock];
-  TravStack st;
-  st.smem = stack_mem + threadIdx.x;
-  st.stride = kBlock;
-  st.sp = 0;
   unsigned status = 0;
   CountQuery q{sc, rays, counts, 0, 0, 0.0f, {}};
-  traverse_persistent(sc, q, n, fetch, st, status);
+  walk<kRefill, kBlock, kShort>(sc, q, n, fetch, status);
   if (status) atomicOr(fetch + 1, status);
 }
 
@@ -1468,19 +1498,14 @@ __global__ void __launch_bounds__(kBlock) k_batch_raygen(const BatchTables* __re
 }
 
 template <int B, int S>
-__global__ void __launch_bounds__(B, 1280 / B) k_batch_extend(DScene sc, int s, BatchTables* t, PathState ps,
+__global__ void __launch_bounds__(B, kExtendBlocks128 * 128 / B) k_batch_extend(DScene sc, int s, BatchTables* t, PathState ps,
                                                     BatchCounters* bc) {
   SceneQueues* sq = &t->scenes[s];
   const int n = static_cast<int>(sq->count);
   if (n == 0) return;
-  __shared__ int stack_mem[S * B];
-  TravStackT<S> st;
-  st.smem = stack_mem + threadIdx.x;
-  st.stride = B;
-  st.sp = 0;
   unsigned status = 0;
   ExtendQuery q{sc, ps, ps.queue[t->iteration & 1] + sq->base, 0, {}};
-  traverse_persistent<kRefillClosest>(sc, q, n, &sq->fetch, st, status);
+  walk<kRefillClosest, B, S>(sc, q, n, &sq->fetch, status);
   if (status) atomicOr(&bc->status, status);
 }
 
@@ -1518,16 +1543,11 @@ __global__ void __launch_bounds__(B, 1152 / B) k_batch_shadow(DScene sc, int s, 
   SceneQueues* sq = &t->scenes[s];
   const int n = static_cast<int>(sq->shadow_count);
   if (n == 0) return;
-  __shared__ int stack_mem[S * B];
-  TravStackT<S> st;
-  st.smem = stack_mem + threadIdx.x;
-  st.stride = B;
-  st.sp = 0;
   unsigned status = 0;
   PathState pq = ps;
   pq.shadow_queue += 3ull * sq->base * static_cast<unsigned>(slots);
   ShadowQuery q{sc, pq, capacity, &status};
-  traverse_persistent<kRefillShadow>(sc, q, n, &sq->fetch_shadow, st, status);
+  walk<kRefillShadow, B, S>(sc, q, n, &sq->fetch_shadow, status);
   if (status) atomicOr(&bc->status, status);
 }
 

@@ -144,10 +144,10 @@ def test_rebuild_frame_with_32_bins_equals_oracle_tree_and_hits():
         rng = np.random.default_rng(9)
         idx = rng.choice(big.width * big.height, 16384, replace=False)
         px, py = (idx % big.width).astype(np.int32), (idx // big.width).astype(np.int32)
-        scene_d = CompiledScene(dev, big.compiled.materials, big.compiled.textures, [], big.compiled.lights,
-                                big.compiled.background, -1, None)
-        scene_o = CompiledScene(o, big.compiled.materials, big.compiled.textures, [], big.compiled.lights,
-                                big.compiled.background, -1, None)
+        scene_d = CompiledScene(dev, big.shading.materials, big.shading.textures, [], big.shading.lights,
+                                big.shading.background, -1, None)
+        scene_o = CompiledScene(o, big.shading.materials, big.shading.textures, [], big.shading.lights,
+                                big.shading.background, -1, None)
         g = ex.trace_primary(scene_d, cam, big.width, big.height, 2, 0, px, py)
         r = cpu.trace_primary(scene_o, cam, big.width, big.height, 2, 0, px, py, threads=8)
         g_in = np.where(g["tri"] >= 0, dev.order[np.maximum(g["tri"], 0)], -1)

@@ -3,12 +3,13 @@
 The reference's walks have no bounds (src/bvh.ts:202-332 keeps an explicit
 stack of 256 entries, and attenuateShadow, src/tracer.ts:557-594, keeps every
 see-through hit in a growing list). The device walks keep a traversal stack
-of 104 entries (the builder's depth limit is 100), a list of 64 distinct
-see-through hits per shadow ray, and a step budget per query; reaching any of
-them ends the query without a fault and sets a status bit, and the call then
-fails with MCRT_ERR_WALK (WalkLimitError) instead of returning an image that
-may differ from the reference's, as the reference's worker turns any failure
-into {type: 'error'} (src/protocol.ts:101-104).
+of bounded depth, a list of 64 distinct see-through hits per shadow ray, and
+a step budget per query; reaching any of them ends the query without a fault
+and sets a status bit, and the call then fails with MCRT_ERR_WALK
+(WalkLimitError) instead of returning an image that may differ from the
+reference's, as the reference's worker turns any failure into
+{type: 'error'} (src/protocol.ts:101-104). A BVH that is not a tree (a
+subtree shared by two parents) is refused when it is sent.
 
 Each case makes one bound run out on a well-formed input (nothing faults or
 waits), checks the error, then renders or traces a normal input on the same
@@ -114,7 +115,10 @@ def _chain_geometry(depth: int) -> CompiledGeometry:
 
 
 def test_bvh_deeper_than_the_traversal_stack_fails(ex):
-    ex.send({"type": "geometry", "version": 1, "geometry": _chain_geometry(110)})
+    # The walk's stack holds one entry per level still to finish: a chain a
+    # thousand levels deep needs more than it has, whichever layout it walks
+    # (binary levels, or wide nodes of up to seven of them).
+    ex.send({"type": "geometry", "version": 1, "geometry": _chain_geometry(1000)})
     ray = np.array([[0.1, 0.1, 500, 0, 0, 0, -1, 0]], np.float32)
     with pytest.raises(WalkLimitError) as err:
         ex.intersect_closest(1, ray)
@@ -123,6 +127,20 @@ def test_bvh_deeper_than_the_traversal_stack_fails(ex):
     ex.send({"type": "geometry", "version": 2, "geometry": _chain_geometry(100)})
     hit = ex.intersect_closest(2, ray)
     assert hit["tri"][0] == 100 and abs(hit["t"][0] - (500 - 100.25)) < 1e-3
+    _still_usable(ex)
+
+
+def test_a_bvh_that_is_not_a_tree_is_refused(ex):
+    """Inner node 0's right child (node 2) has the same children as its left child
+    (node 1): every index points forward, but leaves 3 and 4 are reached twice."""
+    from meercadraytracer_b200._lib import MCRT_ERR_INVALID, McrtError
+
+    g = _chain_geometry(2)  # 3 triangles, nodes 0 (inner), 1 leaf, 2 inner, 3 leaf, 4 leaf
+    nodes = np.array([[1, 0, 2], [3, 0, 2], [3, 0, 2], [0, 2, 0], [2, 1, 0]], np.int32)
+    g.bvh = CompiledBvh(np.tile(g.bvh.bounds.reshape(-1, 6)[0], (5, 1)).reshape(-1), nodes.reshape(-1), 5)
+    with pytest.raises(McrtError) as err:
+        ex.send({"type": "geometry", "version": 3, "geometry": g})
+    assert err.value.code == MCRT_ERR_INVALID and "not a tree" in str(err.value)
     _still_usable(ex)
 
 
