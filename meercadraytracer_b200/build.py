@@ -27,11 +27,9 @@ SOURCES = {
     "render.cu": [],
     "executor.cu": [],
     "batch.cu": [],
-    "wide_bvh.cu": [],
     "scene_build.cu": ["--fmad=false"],
 }
-HEADERS = ["mcrt_math.cuh", "device_scene.cuh", "traverse.cuh", "render.cuh", "scene_build.cuh", "batch.cuh", "dfg_lut.h",
-           "wide_bvh.cuh"]
+HEADERS = ["mcrt_math.cuh", "device_scene.cuh", "traverse.cuh", "render.cuh", "scene_build.cuh", "batch.cuh", "dfg_lut.h"]
 
 
 def nvcc() -> str:

@@ -82,14 +82,11 @@ struct DFog {
 
 struct DScene {
   const DNode* nodes;
-  const uint4* wnodes;   // compressed 8-wide BVH (wide_bvh.cuh), 5 words per node
-  const float4* wtris;   // triangles in wide order, compiled-geometry index in the third w
   const float4* tris;
   const float4* attrs;
   const float4* tangents;
   const float4* colors;  // 3 per triangle, or null
   int tri_count;
-  int wide_nodes;        // nodes of the wide BVH
   int root_count;        // > 0: the root is a leaf of this many triangles (from 0); 0: node 0 is inner
   float eps;             // CompiledGeometry.epsilon
   int node_count;

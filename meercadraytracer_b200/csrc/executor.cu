@@ -27,7 +27,6 @@
 #include "render.cuh"
 #include "scene_build.cuh"
 #include "traverse.cuh"
-#include "wide_bvh.cuh"
 
 namespace mcrt {
 namespace {
@@ -168,14 +167,11 @@ class DevBuf {
 
 struct GeometryGpu {
   DevBuf nodes, tris, attrs, tangents, colors;
-  DevBuf wnodes, wtris;  // the compressed 8-wide BVH the traversal walks, and its triangles
-  int tri_count = 0, root_count = 0, node_count = 0, wide_nodes = 0;
+  int tri_count = 0, root_count = 0, node_count = 0;
   float eps = 1e-7f;
   int64_t max_material = -1;
   bool has_colors = false;
-  size_t bytes() const {
-    return nodes.size() + tris.size() + attrs.size() + tangents.size() + colors.size() + wnodes.size() + wtris.size();
-  }
+  size_t bytes() const { return nodes.size() + tris.size() + attrs.size() + tangents.size() + colors.size(); }
 };
 
 struct TextureGpu {
@@ -214,7 +210,6 @@ struct mcrt_executor {
   double ms_total = 0;
   DevBuf sum, image, list_x, list_y, out_tile, rays, hits, scratch;
   DevBuf pack_flag, pack_index, pack_temp;  // node packing of device-compiled geometry, kept across rebuilds
-  DevBuf wide_items, wide_counters;         // wide BVH build scratch, kept across rebuilds
   DevBuf dfg_buf, srgb_lut;
   cudaTextureObject_t dfg_tex = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -267,14 +262,11 @@ mcrt_executor* checked(mcrt_executor* ex) {
 DScene make_scene(mcrt_executor* ex) {
   DScene s{};
   s.nodes = ex->geo.nodes.as<DNode>();
-  s.wnodes = ex->geo.wnodes.as<uint4>();
-  s.wtris = ex->geo.wtris.as<float4>();
   s.tris = ex->geo.tris.as<float4>();
   s.attrs = ex->geo.attrs.as<float4>();
   s.tangents = ex->geo.tangents.as<float4>();
   s.colors = ex->geo.has_colors ? ex->geo.colors.as<float4>() : nullptr;
   s.tri_count = ex->geo.tri_count;
-  s.wide_nodes = ex->geo.wide_nodes;
   s.root_count = ex->geo.root_count;
   s.eps = ex->geo.eps;
   s.node_count = ex->geo.node_count;
@@ -290,33 +282,6 @@ DScene make_scene(mcrt_executor* ex) {
   s.background = ex->sh.background;
   s.fog = ex->sh.fog;
   return s;
-}
-
-// The compressed 8-wide tree the traversal kernels walk (wide_bvh.cuh), from
-// the binary tree in the reference's layout on the device and the packed
-// triangles; the binary tree itself stays the compiled geometry's.
-void build_wide(mcrt_executor* ex, const int* nodes, const float* bounds) {
-  GeometryGpu& G = ex->geo;
-  G.wide_nodes = 0;
-#ifndef MCRT_BINARY_WALK
-  const int n = G.tri_count;
-  if (n <= 0) return;
-  G.wnodes.ensure(sizeof(uint4) * kWideNodeWords * static_cast<size_t>(n));
-  G.wtris.ensure(sizeof(float4) * 3 * static_cast<size_t>(n));
-  ex->wide_items.ensure(wide_bvh_item_bytes(n));
-  ex->wide_counters.ensure(4 * sizeof(unsigned));
-  int count = 0;
-  const cudaError_t e = build_wide_bvh(nodes, bounds, G.root_count, G.tris.as<float4>(), n, G.wnodes.as<uint4>(),
-                                       G.wtris.as<float4>(), ex->wide_items.as<void>(),
-                                       ex->wide_counters.as<unsigned>(), &count, ex->stream);
-  if (e == cudaErrorInvalidValue)
-    fail(MCRT_ERR_INVALID, "the BVH is not a tree: a node or a triangle is reached from two parents");
-  cuda_check(e, "wide BVH build");
-  G.wide_nodes = count;
-#else
-  (void)nodes;
-  (void)bounds;
-#endif
 }
 
 void require_scene(mcrt_executor* ex, int32_t gv, int32_t sv, bool need_shading) {
@@ -611,9 +576,8 @@ int32_t mcrt_send_geometry(mcrt_executor* ex, int32_t version, const mcrt_geomet
       G.tangents.upload(g->tangents, sizeof(float) * 4 * n, s);
       G.has_colors = g->colors != nullptr;
       if (G.has_colors) G.colors.upload(g->colors, sizeof(float) * 12 * n, s);
-      DevBuf nodes, bounds;
+      DevBuf nodes;
       nodes.upload(g->bvh_nodes, sizeof(int) * 3 * m, s);
-      bounds.upload(g->bvh_bounds, sizeof(float) * 6 * m, s);
       k_mark_leaf_ends<<<blocks(m, 256), 256, 0, s>>>(nodes.as<int>(), m, G.tris.as<float4>());
       if (G.root_count == 0) {
         // Inner nodes numbered depth first (preorder, left child first): a
@@ -633,7 +597,8 @@ int32_t mcrt_send_geometry(mcrt_executor* ex, int32_t version, const mcrt_geomet
           todo.push_back(first + 1);
           todo.push_back(first);
         }
-        DevBuf index;
+        DevBuf bounds, index;
+        bounds.upload(g->bvh_bounds, sizeof(float) * 6 * m, s);
         index.upload(order_index.data(), sizeof(int) * m, s);
         G.nodes.ensure(sizeof(DNode) * std::max(inner, 1));
         k_pack_nodes<<<blocks(m, 256), 256, 0, s>>>(bounds.as<float>(), nodes.as<int>(), index.as<int>(), m,
@@ -644,9 +609,6 @@ int32_t mcrt_send_geometry(mcrt_executor* ex, int32_t version, const mcrt_geomet
         cuda_check(cudaGetLastError(), "geometry conversion");
         cuda_check(cudaStreamSynchronize(s), "geometry upload");
       }
-      build_wide(ex, nodes.as<int>(), bounds.as<float>());
-    } else {
-      G.wide_nodes = 0;
     }
     ex->geometry_version = version;
     ex->have_geometry = true;
@@ -1160,9 +1122,6 @@ int32_t mcrt_compile_instances(mcrt_executor* ex, int32_t version, int32_t count
         cuda_check(cudaGetLastError(), "BVH conversion");
         cuda_check(cudaStreamSynchronize(s), "geometry pack");
       }
-      build_wide(ex, g.nodes, g.bounds);
-    } else {
-      G.wide_nodes = 0;
     }
     cuda_check(cudaGetLastError(), "geometry pack");
     if (out) {

@@ -50,34 +50,17 @@ MCRT_D unsigned int queue_append(unsigned int* counter) {
 }
 
 // ------------------------------------------------------------------- walks
-// The traversal every query kernel runs: the compressed 8-wide BVH, or the
-// binary tree when built with MCRT_BINARY_WALK. B threads per block, S
-// shared-memory stack entries per thread, warps refilled once REFILL lanes
-// are idle.
-#ifdef MCRT_BINARY_WALK
-constexpr bool kWideWalk = false;
-#else
-constexpr bool kWideWalk = true;
-#endif
-constexpr int kPostpone = 8;  // wide walk: triangle tests postponed while fewer lanes than this test triangles
-
+// The traversal every query kernel runs (traverse_persistent): B threads per
+// block, S shared-memory stack entries per thread, warps refilled once REFILL
+// lanes are idle.
 template <int REFILL, int B, int S, class Q>
 MCRT_D void walk(const DScene& sc, Q& q, int n, unsigned* counter, unsigned& status) {
-  if constexpr (kWideWalk) {
-    __shared__ uint2 wide_stack[S * B];
-    WideStackT<S> st;
-    st.smem = wide_stack + threadIdx.x;
-    st.stride = B;
-    st.sp = 0;
-    traverse_wide<REFILL, kPostpone>(sc, q, n, counter, st, status);
-  } else {
-    __shared__ int binary_stack[S * B];
-    TravStackT<S> st;
-    st.smem = binary_stack + threadIdx.x;
-    st.stride = B;
-    st.sp = 0;
-    traverse_persistent<REFILL>(sc, q, n, counter, st, status);
-  }
+  __shared__ int stack[S * B];
+  TravStackT<S> st;
+  st.smem = stack + threadIdx.x;
+  st.stride = B;
+  st.sp = 0;
+  traverse_persistent<REFILL>(sc, q, n, counter, st, status);
 }
 
 // ---------------------------------------------------------------- mapping
@@ -173,7 +156,6 @@ struct ExtendQuery {
   MCRT_D const TravRay& ray() const { return cs.r; }
   MCRT_D float t_max() const { return cs.tmax; }
   MCRT_D bool leaf(int first) { return cs.leaf(sc, first); }
-  MCRT_D bool tri(int k) { return cs.wide_tri(sc, k); }
   MCRT_D void finish() {
     const ClosestHit& h = cs.h;
     const unsigned word = h.tri >= 0 ? ((h.front ? 0x80000000u : 0u) | static_cast<unsigned>(h.tri + 1)) : 0u;
@@ -182,12 +164,10 @@ struct ExtendQuery {
 };
 
 // B threads per block, S short-stack entries per thread (a traversal variant).
-// kExtendBlocks128 blocks of 128 threads per SM set the register cap: the
-// binary walk at 10 (48 registers, a few bytes of spills, a ninth more
-// resident warps than its unconstrained 56); the wide walk at 9 (56).
-constexpr int kExtendBlocks128 = kWideWalk ? 9 : 10;
+// 1280 / B blocks per SM: the register cap (48) costs a few bytes of spills
+// and buys a ninth more resident warps than the unconstrained 56 registers.
 template <int B, int S>
-__global__ void __launch_bounds__(B, kExtendBlocks128 * 128 / B) k_extend(DScene sc, PathState ps, const int* __restrict__ queue, int n,
+__global__ void __launch_bounds__(B, 1280 / B) k_extend(DScene sc, PathState ps, const int* __restrict__ queue, int n,
                                               Counters* cnt) {
   unsigned status = 0;
   ExtendQuery q{sc, ps, queue, 0, {}};
@@ -840,14 +820,6 @@ struct ShadowQuery {
     }
     return true;
   }
-  // Wide-order triangle k; false once the ray is blocked.
-  MCRT_D bool tri(int k) {
-    const float4* p = sc.wtris + 3 * static_cast<size_t>(k);
-    const float4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2);
-    TriHit th;
-    return !(intersect_triangle(r, V3{w0.x, w0.y, w0.z}, V3{w1.x, w1.y, w1.z}, V3{w2.x, w2.y, w2.z}, max_t, 2, th) &&
-             visit(__float_as_int(w2.w), th, w0, w1));
-  }
   // One hit of the visitor; true once the ray is blocked.
   MCRT_D bool visit(int k, const TriHit& th, float4 w0, float4 w1) {
     const int fl = tri_flags(w0.w);
@@ -1040,7 +1012,6 @@ struct RayQuery {
   MCRT_D const TravRay& ray() const { return cs.r; }
   MCRT_D float t_max() const { return cs.tmax; }
   MCRT_D bool leaf(int first) { return cs.leaf(sc, first); }
-  MCRT_D bool tri(int k) { return cs.wide_tri(sc, k); }
   MCRT_D void finish() {
     hits[i] = make_int4(cs.h.tri, __float_as_int(cs.h.t), __float_as_int(cs.h.u),
                         (cs.h.front ? 1 : 0) | (min(cs.tests, 0xffffff) << 8));
@@ -1081,13 +1052,6 @@ struct CountQuery {
       if (intersect_triangle(r, a, b, c, limit, 2, th)) hits++;
       if (leaf_end(w0.w)) break;
     }
-    return true;
-  }
-  MCRT_D bool tri(int k) {
-    const float4* p = sc.wtris + 3 * static_cast<size_t>(k);
-    const float4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2);
-    TriHit th;
-    if (intersect_triangle(r, V3{w0.x, w0.y, w0.z}, V3{w1.x, w1.y, w1.z}, V3{w2.x, w2.y, w2.z}, limit, 2, th)) hits++;
     return true;
   }
   MCRT_D void finish() { counts[i] = hits; }
@@ -1498,7 +1462,7 @@ __global__ void __launch_bounds__(kBlock) k_batch_raygen(const BatchTables* __re
 }
 
 template <int B, int S>
-__global__ void __launch_bounds__(B, kExtendBlocks128 * 128 / B) k_batch_extend(DScene sc, int s, BatchTables* t, PathState ps,
+__global__ void __launch_bounds__(B, 1280 / B) k_batch_extend(DScene sc, int s, BatchTables* t, PathState ps,
                                                     BatchCounters* bc) {
   SceneQueues* sq = &t->scenes[s];
   const int n = static_cast<int>(sq->count);

@@ -48,7 +48,7 @@ constexpr int kRefillShadow = 20;
 constexpr unsigned kStatusStackOverflow = 1u;
 constexpr unsigned kStatusShadowListOverflow = 2u;
 constexpr unsigned kStatusStepLimit = 4u;  // a query hit the step budget and was ended
-constexpr unsigned kStatusLeafRange = 8u;  // a leaf ran past the last triangle (or a wide node's index past the end)
+constexpr unsigned kStatusLeafRange = 8u;  // a leaf ran past the last triangle and was cut
 
 // Node visits plus leaves one query may take: a walk of a well-formed BVH of
 // N triangles enters each of its fewer than 2N nodes at most once, so past
@@ -135,7 +135,9 @@ MCRT_D float box_entry(const TravRay& r, float x0, float x1, float y0, float y1,
   float ty0 = (y0 - r.o.y) * r.inv.y, ty1 = (y1 - r.o.y) * r.inv.y;
   float tz0 = (z0 - r.o.z) * r.inv.z, tz1 = (z1 - r.o.z) * r.inv.z;
   float lo = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
-  float hi = fminf(fminf(fmaxf(tx0, tx1) * g, fmaxf(ty0, ty1) * g), fminf(fmaxf(tz0, tz1) * g, t_max));
+  // Each exit scaled by g, then the least: rounding x * g is monotone in x, so
+  // scaling the least exit once gives the same value.
+  float hi = fminf(fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1)) * g, t_max);
   return lo <= hi ? lo : -1.0f;
 }
 
@@ -314,208 +316,6 @@ MCRT_D void traverse_persistent(const DScene& sc, Q& q, int n, unsigned* counter
   }
 }
 
-// ------------------------------------------------------------ wide layout
-// Traversal of the compressed 8-wide BVH (wide_bvh.cuh), after Ylitie,
-// Karras and Laine (HPG 2017). A lane holds a node group (child_base; the
-// hit bits of the node children still to visit in bits 24-31, ordered near
-// to far by the ray's octant, and the node's imask in bits 0-7) and a
-// triangle group (tri_base; a 24-bit mask of triangles still to test). It
-// visits the nearest child of its node group, pushing the rest of the group,
-// tests that child's eight boxes at once and makes its hits the new groups;
-// then it tests the triangle group, postponing it (pushed, for later) while
-// fewer than POSTPONE lanes of the warp are testing triangles and it still
-// has node children to visit, so the warp's lanes keep walking nodes
-// together. Persistent, with warps refilled from a
-// global counter as in traverse_persistent.
-//
-// The box test decodes each child plane as p + q 2^e, and its distance along
-// the ray as q (2^e / d) + (p - o) / d with one fused multiply-add rounded
-// down (entry) or up (exit), after widening (p - o) / d by a bound on its own
-// rounding: an entry distance is never above, an exit distance never below
-// the exact value for the float ray, so no box the ray touches is missed
-// (the flat boxes of planes included, as the reference's boxEntry accepts
-// them, src/bvh.ts:340-356).
-constexpr int kWideStackMax = 128;
-
-template <int SHORT>
-struct WideStackT {
-  static_assert(SHORT > 0 && SHORT < kWideStackMax, "short stack depth out of range");
-  uint2* smem;  // this thread's column: entry i at smem[i * stride]
-  int stride;
-  int sp;
-  uint2 spill[kWideStackMax - SHORT];
-  MCRT_D bool push(uint2 v) {
-    if (sp < SHORT) {
-      smem[sp * stride] = v;
-    } else if (sp < kWideStackMax) {
-      spill[sp - SHORT] = v;
-    } else {
-      return false;
-    }
-    sp++;
-    return true;
-  }
-  MCRT_D uint2 pop() {
-    --sp;
-    return sp < SHORT ? smem[sp * stride] : spill[sp - SHORT];
-  }
-};
-
-// Grid coordinate j (0-3) of a word of four bytes, as a float.
-MCRT_D float grid_byte(unsigned w, unsigned j) {
-  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | j)) - 8388608.0f;
-}
-
-// Octant swizzle of a ray: xor with a slot gives its hit bit's order, nearest
-// slot first (slot bit a set for children below the centre on axis a).
-MCRT_D unsigned ray_octant_swizzle(const TravRay& r) {
-  return 7u ^ ((r.inv.x < 0.0f ? 1u : 0u) | (r.inv.y < 0.0f ? 2u : 0u) | (r.inv.z < 0.0f ? 4u : 0u));
-}
-
-// Tests the eight children of wide node `index` and returns the node and
-// triangle groups of those the ray enters before t_max.
-MCRT_D void wide_node_hits(const uint4* __restrict__ wnodes, int index, const TravRay& r, unsigned swz, float t_max,
-                           uint2& ng, uint2& tg) {
-  const uint4* p = wnodes + 5 * static_cast<size_t>(index);
-  const uint4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2), w3 = __ldg(p + 3), w4 = __ldg(p + 4);
-  const float adjx = r.inv.x * __uint_as_float((w0.w & 0xffu) << 23);
-  const float adjy = r.inv.y * __uint_as_float(((w0.w >> 8) & 0xffu) << 23);
-  const float adjz = r.inv.z * __uint_as_float(((w0.w >> 16) & 0xffu) << 23);
-  const float ox = (__uint_as_float(w0.x) - r.o.x) * r.inv.x;
-  const float oy = (__uint_as_float(w0.y) - r.o.y) * r.inv.y;
-  const float oz = (__uint_as_float(w0.z) - r.o.z) * r.inv.z;
-  // Two roundings made ox: 2^-22 |ox| bounds their error.
-  const float ex = fabsf(ox) * 2.384185791e-7f, ey = fabsf(oy) * 2.384185791e-7f, ez = fabsf(oz) * 2.384185791e-7f;
-  const float nox = __fsub_rd(ox, ex), noy = __fsub_rd(oy, ey), noz = __fsub_rd(oz, ez);
-  const float fox = __fadd_ru(ox, ex), foy = __fadd_ru(oy, ey), foz = __fadd_ru(oz, ez);
-  // Entry planes are the low ones for a positive direction, the high ones otherwise.
-  const bool sx = r.inv.x < 0.0f, sy = r.inv.y < 0.0f, sz = r.inv.z < 0.0f;
-  const unsigned nx0 = sx ? w3.z : w2.x, nx1 = sx ? w3.w : w2.y, fx0 = sx ? w2.x : w3.z, fx1 = sx ? w2.y : w3.w;
-  const unsigned ny0 = sy ? w4.x : w2.z, ny1 = sy ? w4.y : w2.w, fy0 = sy ? w2.z : w4.x, fy1 = sy ? w2.w : w4.y;
-  const unsigned nz0 = sz ? w4.z : w3.x, nz1 = sz ? w4.w : w3.y, fz0 = sz ? w3.x : w4.z, fz1 = sz ? w3.y : w4.w;
-  unsigned hits = 0;
-#pragma unroll
-  for (unsigned c = 0; c < 8; c++) {
-    const unsigned j = c & 3u;
-    const bool hi = c >= 4;
-    const float tnx = __fmaf_rd(grid_byte(hi ? nx1 : nx0, j), adjx, nox);
-    const float tny = __fmaf_rd(grid_byte(hi ? ny1 : ny0, j), adjy, noy);
-    const float tnz = __fmaf_rd(grid_byte(hi ? nz1 : nz0, j), adjz, noz);
-    const float tfx = __fmaf_ru(grid_byte(hi ? fx1 : fx0, j), adjx, fox);
-    const float tfy = __fmaf_ru(grid_byte(hi ? fy1 : fy0, j), adjy, foy);
-    const float tfz = __fmaf_ru(grid_byte(hi ? fz1 : fz0, j), adjz, foz);
-    const float enter = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
-    const float leave = fminf(fminf(tfx, tfy), fminf(tfz, t_max));
-    // The float ray's inverse direction itself is rounded: allow 2^-20 relative.
-    if (enter <= leave * 1.00000095f) {
-      const unsigned m = ((hi ? w1.w : w1.z) >> (8 * j)) & 0xffu;
-      const unsigned inner = (m & (m << 1)) & 0x10u;
-      hits |= (m >> 5) << ((m & 0x1fu) ^ (inner ? swz : 0u));
-    }
-  }
-  ng = make_uint2(w1.x, (hits & 0xff000000u) | (w0.w >> 24));
-  tg = make_uint2(w1.y, hits & 0x00ffffffu);
-}
-
-// Persistent traversal of queries [0, n) over the wide BVH. Q supplies, per
-// lane: load(index), ray(), t_max(), finish() as for traverse_persistent,
-// and bool tri(int k): test wide-order triangle k (false ends the query).
-template <int REFILL, int POSTPONE, class Q, class ST>
-MCRT_D void traverse_wide(const DScene& sc, Q& q, int n, unsigned* counter, ST& st, unsigned& status) {
-  const unsigned lane = threadIdx.x & 31;
-  const bool empty = sc.tri_count == 0;
-  const int step_limit = max_steps(sc);
-  uint2 ng = make_uint2(0u, 0u), tg = make_uint2(0u, 0u);
-  unsigned swz = 0;
-  int steps = 0;
-  bool has = false;
-  bool exhausted = false;
-  for (;;) {
-    const bool need = !has && !exhausted;
-    const unsigned mneed = __ballot_sync(0xffffffffu, need);
-    if (mneed) {
-      const int leader = __ffs(mneed) - 1;
-      unsigned base = 0;
-      if (static_cast<int>(lane) == leader) base = atomicAdd(counter, __popc(mneed));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      if (need) {
-        const unsigned idx = base + __popc(mneed & lanemask_lt());
-        if (idx < static_cast<unsigned>(n)) {
-          q.load(static_cast<int>(idx));
-          has = true;
-          st.sp = 0;
-          steps = 0;
-          swz = ray_octant_swizzle(q.ray());
-          ng = make_uint2(0u, empty ? 0u : (1u << 24));  // the root, wide node 0
-          tg = make_uint2(0u, 0u);
-        } else {
-          exhausted = true;
-        }
-      }
-    }
-    if (__all_sync(0xffffffffu, !has)) return;
-    do {
-      if (has) {
-        if (ng.y & 0xff000000u) {
-          const unsigned b = static_cast<unsigned>(__ffs(ng.y >> 24)) + 23u;
-          ng.y &= ~(1u << b);
-          const unsigned slot = (b - 24u) ^ swz;
-          const int child = static_cast<int>(ng.x) + __popc(ng.y & ((1u << slot) - 1u) & 0xffu);
-          if ((ng.y & 0xff000000u) && !st.push(ng)) status |= kStatusStackOverflow;
-          if (++steps > step_limit) {
-            status |= kStatusStepLimit;
-            ng = tg = make_uint2(0u, 0u);
-            st.sp = 0;
-          } else if (child >= sc.wide_nodes) {
-            status |= kStatusLeafRange;  // never for a tree the builder made; skipped, not read
-            ng = tg = make_uint2(0u, 0u);
-          } else {
-            wide_node_hits(sc.wnodes, child, q.ray(), swz, q.t_max(), ng, tg);
-          }
-        } else {
-          tg = ng;  // a triangle group taken from the stack (or nothing)
-          ng = make_uint2(0u, 0u);
-        }
-        while (tg.y) {
-          // Postponed only while the lane has node children left: the next
-          // iteration then visits a node, so every iteration makes progress
-          // (a node visit, or a whole triangle group tested).
-          if ((ng.y & 0xff000000u) && __popc(__activemask()) < POSTPONE) {
-            if (!st.push(tg)) status |= kStatusStackOverflow;
-            tg.y = 0;
-            break;
-          }
-          const int k = __ffs(tg.y) - 1;
-          tg.y &= tg.y - 1;
-          if (++steps > step_limit) {
-            status |= kStatusStepLimit;
-            ng = tg = make_uint2(0u, 0u);
-            st.sp = 0;
-            break;
-          }
-          if (static_cast<int>(tg.x) + k >= sc.tri_count) {
-            status |= kStatusLeafRange;  // as above
-            continue;
-          }
-          if (!q.tri(static_cast<int>(tg.x) + k)) {
-            ng = tg = make_uint2(0u, 0u);
-            st.sp = 0;
-            break;
-          }
-        }
-        if (!(ng.y & 0xff000000u)) {
-          if (st.sp > 0) {
-            ng = st.pop();
-          } else {
-            q.finish();
-            has = false;
-          }
-        }
-      }
-    } while (__popc(__ballot_sync(0xffffffffu, !has)) < REFILL && __any_sync(0xffffffffu, has));
-  }
-}
-
 // Closest hit of one query: intersectClosest, src/bvh.ts:202-282.
 struct ClosestHit {
   int tri;
@@ -548,19 +348,6 @@ struct ClosestState {
         h = ClosestHit{k, th.t, th.u, th.v, th.front};
       }
       if (leaf_end(w0.w)) break;
-    }
-    return true;
-  }
-  // Wide-order triangle k; a hit records the compiled geometry's index.
-  MCRT_D bool wide_tri(const DScene& sc, int k) {
-    const float4* p = sc.wtris + 3 * static_cast<size_t>(k);
-    const float4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2);
-    tests++;
-    TriHit th;
-    if (intersect_triangle(r, V3{w0.x, w0.y, w0.z}, V3{w1.x, w1.y, w1.z}, V3{w2.x, w2.y, w2.z}, tmax,
-                           cull ? tri_side(w0.w) : 2, th)) {
-      tmax = th.t;
-      h = ClosestHit{__float_as_int(w2.w), th.t, th.u, th.v, th.front};
     }
     return true;
   }
