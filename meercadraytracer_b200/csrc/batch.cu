@@ -263,7 +263,9 @@ bool BatchEngine::admit(Request& r) {
 
 // Chooses the chunk's segments: admissions in submission order while the
 // arena has room, previews first, then passes of the admitted requests in
-// submission order, each request at most once.
+// submission order, each request at most once: whole passes where they fit,
+// else a pixel range of the next pass that fills the room.
+constexpr int kMinFragment = 1 << 16;
 void BatchEngine::plan(Chunk& c) {
   long long room = chunk_paths_ > 0 ? std::min(chunk_paths_, capacity_) : capacity_;
   for (auto& rp : requests_) {
@@ -284,7 +286,9 @@ void BatchEngine::plan(Chunk& c) {
     if (!active(r) || r.preview != 1 || static_cast<int>(c.segs.size()) >= kMaxSegments) continue;
     const int b = r.d.preview_block;
     const long long blocks = static_cast<long long>((r.d.fp.width + b - 1) / b) * ((r.d.fp.height + b - 1) / b);
-    if (blocks > room) continue;
+    // A preview larger than the chunk size (never than the pool: submission
+    // checks) goes alone into an empty chunk.
+    if (blocks > room && !(c.segs.empty() && blocks <= capacity_)) continue;
     take(r, 1, 0, 1, 0, static_cast<int>(blocks));
     r.preview = 2;
   }
@@ -294,10 +298,14 @@ void BatchEngine::plan(Chunk& c) {
     if (std::find(used.begin(), used.end(), &r) != used.end()) continue;
     if (r.next_pass >= r.d.samples || room <= 0) continue;
     const long long P = r.pixels();
-    if (r.next_pix > 0 || P > capacity_) {
-      // A pass larger than the pool, or one already split: the next pixel range.
+    if (r.next_pix > 0 || P > room) {
+      // A pass larger than the room left in this chunk, or one already split:
+      // the next pixel range, so chunks run full. A range shorter than
+      // kMinFragment that does not end the pass waits for the next chunk,
+      // unless nothing else is in this one (a chunk smaller than
+      // kMinFragment still makes progress).
       const int n = static_cast<int>(std::min<long long>(room, P - r.next_pix));
-      if (n <= 0) continue;
+      if (n <= 0 || (n < kMinFragment && n < P - r.next_pix && !c.segs.empty())) continue;
       take(r, 0, r.next_pass, 1, r.next_pix, n);
       r.next_pix += n;
       if (r.next_pix >= P) {
@@ -464,10 +472,11 @@ cudaError_t BatchEngine::finish(Chunk& c, std::vector<BatchEvent>& events) {
   return cudaSuccess;
 }
 
-cudaError_t BatchEngine::step(std::vector<BatchEvent>& events, bool* idle) {
+cudaError_t BatchEngine::step(std::vector<BatchEvent>& events, bool* idle, bool* progressed) {
   cudaError_t e = cudaSetDevice(device_);
   if (e != cudaSuccess) return e;
   bool launched = false;
+  if (progressed) *progressed = !inflight_.empty();  // a chunk in flight is finished below
   if (inflight_.size() < 2) {
     Chunk c;
     c.slot = next_slot_;
@@ -478,6 +487,7 @@ cudaError_t BatchEngine::step(std::vector<BatchEvent>& events, bool* idle) {
       e = launch(inflight_.back());
       if (e != cudaSuccess) return e;
       launched = true;
+      if (progressed) *progressed = true;
     }
   }
   if (!inflight_.empty() && (inflight_.size() == 2 || !launched)) {

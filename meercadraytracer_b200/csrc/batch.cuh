@@ -89,8 +89,10 @@ class BatchEngine {
   bool cancel(long long id);
   // Launches the next chunk (if any request has work), then waits for the
   // chunk before it and appends the events it completed. *idle: nothing is
-  // queued, active or in flight.
-  cudaError_t step(std::vector<BatchEvent>& events, bool* idle);
+  // queued, active or in flight. *progressed (if given): a chunk was launched
+  // or finished; a step that does neither while not idle is a scheduling
+  // fault, which callers report instead of stepping again.
+  cudaError_t step(std::vector<BatchEvent>& events, bool* idle, bool* progressed = nullptr);
   BatchTotals totals() const { return totals_; }
   int capacity() const { return capacity_; }
   size_t path_bytes() const { return paths_.bytes(); }

@@ -1316,6 +1316,12 @@ int64_t submit_request(mcrt_batch* b, const mcrt_request* r) {
   const size_t pix = static_cast<size_t>(r->width) * r->height;
   if (pix * 20 + 512 > b->engine.arena().capacity())
     fail(MCRT_ERR_LIMIT, "the request's buffers exceed the batch's memory budget");
+  if (d.preview_block > 1) {
+    const long long blocks = static_cast<long long>((r->width + d.preview_block - 1) / d.preview_block) *
+                             ((r->height + d.preview_block - 1) / d.preview_block);
+    if (blocks > b->engine.capacity())
+      fail(MCRT_ERR_LIMIT, "the block preview needs more paths than the batch's path pool holds");
+  }
   d.scene = scene_slot(b, r);
   const long long id = b->engine.submit(d, r->image, r->preview_image, r->progress_image);
   if (id < 0) fail(MCRT_ERR_INVALID, "request rejected");
@@ -1389,9 +1395,10 @@ int32_t mcrt_batch_step(mcrt_batch* b, mcrt_batch_event* events, int32_t max_eve
     if (max_events < 0 || (max_events > 0 && !events)) fail(MCRT_ERR_INVALID, "bad event buffer");
     check_slots(b);
     std::vector<BatchEvent> ev;
-    bool is_idle = false;
+    bool is_idle = false, progressed = false;
     const unsigned earlier = b->engine.totals().status;
-    cuda_check(b->engine.step(ev, &is_idle), "batch step");
+    cuda_check(b->engine.step(ev, &is_idle, &progressed), "batch step");
+    if (!is_idle && !progressed) fail(MCRT_ERR_LIMIT, "the batch engine could not schedule a pending request");
     if (b->engine.totals().status & kStatusIterationLimit)
       fail(MCRT_ERR_CUDA, "a batched chunk did not finish within its iteration limit");
     check_walk(b->engine.totals().status & ~earlier);
@@ -1412,15 +1419,17 @@ int32_t mcrt_batch_render(mcrt_batch* b, int32_t count, const mcrt_request* requ
     checked_batch(b);
     if (count < 0 || (count > 0 && !requests)) fail(MCRT_ERR_INVALID, "bad request list");
     for (int i = 0; i < count; i++) submit_request(b, requests + i);
-    // Every chunk makes progress or the engine is idle, so this loop ends;
-    // the bound only guards against a scheduling fault.
+    // Every step launches or finishes a chunk until the engine is idle, so
+    // this loop ends; a step that does neither is a scheduling fault and fails
+    // the call rather than spinning.
     bool idle = false;
-    for (long long guard_steps = 0; !idle; guard_steps++) {
-      if (guard_steps > (1LL << 40)) fail(MCRT_ERR_LIMIT, "batch did not finish");
+    while (!idle) {
       check_slots(b);
       std::vector<BatchEvent> ev;
       const unsigned earlier = b->engine.totals().status;
-      cuda_check(b->engine.step(ev, &idle), "batch step");
+      bool progressed = false;
+      cuda_check(b->engine.step(ev, &idle, &progressed), "batch step");
+      if (!idle && !progressed) fail(MCRT_ERR_LIMIT, "the batch engine could not schedule a pending request");
       if (b->engine.totals().status & kStatusIterationLimit)
         fail(MCRT_ERR_CUDA, "a batched chunk did not finish within its iteration limit");
       check_walk(b->engine.totals().status & ~earlier);

@@ -150,8 +150,9 @@ def test_rebuild_frame_with_32_bins_equals_oracle_tree_and_hits():
                                 big.shading.background, -1, None)
         g = ex.trace_primary(scene_d, cam, big.width, big.height, 2, 0, px, py)
         r = cpu.trace_primary(scene_o, cam, big.width, big.height, 2, 0, px, py, threads=8)
-        g_in = np.where(g["tri"] >= 0, dev.order[np.maximum(g["tri"], 0)], -1)
-        r_in = np.where(r["tri"] >= 0, o.order[np.maximum(r["tri"], 0)], -1)
+        # Input-order triangle of each hit, -1 for a miss (int64: `order` is uint32).
+        g_in = np.where(g["tri"] >= 0, dev.order.astype(np.int64)[np.maximum(g["tri"], 0)], -1)
+        r_in = np.where(r["tri"] >= 0, o.order.astype(np.int64)[np.maximum(r["tri"], 0)], -1)
         same = g_in == r_in
         hit = r_in >= 0
         ties = ~same & (g_in >= 0) & hit & (np.abs(g["t"] - r["t"]) <= 1e-5 * np.abs(r["t"]))
