@@ -303,7 +303,7 @@ typedef struct mcrt_batch_event {
 
 typedef struct mcrt_batch_stats {
   uint64_t closest_rays, any_rays, samples, chunks, graph_launches;
-  double gpu_ms;        /* device time of the chunks */
+  double gpu_ms;        /* device time of the chunks, overlapping chunks counted once */
   uint64_t arena_bytes; /* budget for request buffers (sums and images) */
   uint64_t arena_used;
   uint64_t path_bytes;  /* path pool */
@@ -311,14 +311,17 @@ typedef struct mcrt_batch_stats {
   uint32_t pad_;
 } mcrt_batch_stats;
 
-/* A batch renderer on `device`: `capacity` paths per chunk, `arena_bytes` of
- * device memory for admitted requests' sums and images (admission waits for
- * room), `use_graph` 1 to run each chunk's bounce loop as one CUDA graph with
- * a while node, 0 for a host-driven loop. */
+/* A batch renderer on `device`: a pool of `capacity` (at least 2) paths that
+ * two chunks in flight share half and half (one chunk's last, slowest paths
+ * overlap the other's work), `arena_bytes` of device memory for admitted
+ * requests' sums and images (admission waits for room), `use_graph` 1 to run
+ * each chunk's bounce loop as one CUDA graph with a while node, 0 for a
+ * host-driven loop. */
 int32_t mcrt_batch_create(int32_t device, int32_t capacity, int64_t arena_bytes, int32_t use_graph,
                           mcrt_batch** out);
 int32_t mcrt_batch_destroy(mcrt_batch* batch);
-/* Paths per chunk (<= capacity); smaller chunks bound preview latency. */
+/* Paths per chunk (at most half the pool; 0: half the pool); smaller chunks
+ * bound preview latency. */
 int32_t mcrt_batch_set_chunk(mcrt_batch* batch, int32_t paths);
 /* As mcrt_set_traversal, for the batch's kernels. */
 int32_t mcrt_batch_set_traversal(mcrt_batch* batch, int32_t block, int32_t stack);

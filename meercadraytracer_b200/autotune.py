@@ -164,7 +164,8 @@ def tune_batch(renderer: Any, requests: Sequence[Any], chunks: Optional[Sequence
         tv[(b, s)] = timed()
     block, stack = _best(tv)
     renderer.set_traversal(block, stack)
-    chunks = [c for c in (chunks or (capacity // 4, capacity // 2, capacity)) if 0 < c <= capacity]
+    half = capacity // 2  # two chunks share the pool
+    chunks = [c for c in (chunks or (half // 4, half // 2, half)) if 0 < c <= half]
     tc: Dict[int, float] = {}
     for c in chunks:
         renderer.set_chunk(c)
@@ -181,10 +182,10 @@ def tune_batch(renderer: Any, requests: Sequence[Any], chunks: Optional[Sequence
 def tune_serving_chunk(renderer: Any, probes: Sequence[Any], target_ms: float = 12.0, key: Optional[str] = None,
                        cache_path: Optional[str] = None) -> Choice:
     """The serving loop's chunk size: each probe request (one per resident scene, one pass of
-    the served resolution) is timed alone at the engine's full pool; the chunk is the number
-    of paths the slowest scene traces in `target_ms`, rounded down to a multiple of 65,536
-    (at least 262,144, at most the pool)."""
-    capacity = int(renderer.capacity)
+    the served resolution) is timed alone with chunks of half the pool (two chunks share it);
+    the chunk is the number of paths the slowest scene traces in `target_ms`, rounded down to
+    a multiple of 65,536 (at least 262,144, at most half the pool)."""
+    capacity = int(renderer.capacity) // 2
     key = key or f"serve|{device_name(renderer.device)}|{capacity}|{target_ms}|" + ",".join(
         f"{r.scene.geometry.triangle_count}:{r.width}x{r.height}x{r.samples}" for r in probes)
     hit = _load(cache_path, key)

@@ -70,53 +70,93 @@ void DeviceArena::free(void* p) {
 // ----------------------------------------------------------------- engine
 BatchEngine::~BatchEngine() {
   cudaSetDevice(device_);
-  if (stream_) cudaStreamSynchronize(stream_);
+  for (cudaStream_t st : stream_)
+    if (st) cudaStreamSynchronize(st);
   if (copy_stream_) cudaStreamSynchronize(copy_stream_);
   for (Chunk& c : inflight_) {
     if (c.start) cudaEventDestroy(c.start);
     if (c.done) cudaEventDestroy(c.done);
     if (c.copied) cudaEventDestroy(c.copied);
   }
+  if (held_done_) cudaEventDestroy(held_done_);
   if (last_copy_) cudaEventDestroy(last_copy_);
+  if (accumulated_) cudaEventDestroy(accumulated_);
   for (int i = 0; i < kMaxBatchScenes; i++) {
     if (lanes_.stream[i]) cudaStreamDestroy(lanes_.stream[i]);
     if (lanes_.join[i]) cudaEventDestroy(lanes_.join[i]);
   }
   if (lanes_.fork) cudaEventDestroy(lanes_.fork);
-  destroy_graph();
-  if (tables_dev_) cudaFree(tables_dev_);
-  for (BatchTables* t : tables_host_)
-    if (t) cudaFreeHost(t);
-  if (counters_dev_) cudaFree(counters_dev_);
-  if (counters_host_) cudaFreeHost(counters_host_);
-  if (stream_) cudaStreamDestroy(stream_);
+  destroy_graphs();
+  for (int k = 0; k < kSlots; k++) {
+    if (tables_dev_[k]) cudaFree(tables_dev_[k]);
+    if (tables_host_[k]) cudaFreeHost(tables_host_[k]);
+    if (counters_dev_[k]) cudaFree(counters_dev_[k]);
+    if (counters_host_[k]) cudaFreeHost(counters_host_[k]);
+    if (stream_[k]) cudaStreamDestroy(stream_[k]);
+  }
+  if (bins1_) cudaFree(bins1_);
   if (copy_stream_) cudaStreamDestroy(copy_stream_);
 }
 
 cudaError_t BatchEngine::init(int device, int capacity, size_t arena_bytes, bool use_graph) {
   device_ = device;
-  capacity_ = std::max(capacity, 1);
+  capacity_ = std::max(capacity, 2);
+  half_ = capacity_ / 2;
   use_graph_ = use_graph;
   cudaError_t e = cudaSetDevice(device);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+  for (int k = 0; k < kSlots && e == cudaSuccess; k++) e = cudaStreamCreateWithFlags(&stream_[k], cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&last_copy_, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&accumulated_, cudaEventDisableTiming);
   for (int i = 0; i < kMaxBatchScenes && e == cudaSuccess; i++) {
     e = cudaStreamCreateWithFlags(&lanes_.stream[i], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&lanes_.join[i], cudaEventDisableTiming);
   }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&lanes_.fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = arena_.init(arena_bytes);
-  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&tables_dev_), sizeof(BatchTables));
-  for (int i = 0; i < 2 && e == cudaSuccess; i++)
-    e = cudaMallocHost(reinterpret_cast<void**>(&tables_host_[i]), sizeof(BatchTables));
-  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&counters_dev_), sizeof(BatchCounters));
-  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&counters_host_), sizeof(BatchCounters));
-  if (e == cudaSuccess) e = cudaMemset(counters_dev_, 0, sizeof(BatchCounters));
-  if (e == cudaSuccess) e = cudaMemset(tables_dev_, 0, sizeof(BatchTables));
+  for (int k = 0; k < kSlots && e == cudaSuccess; k++) {
+    e = cudaMalloc(reinterpret_cast<void**>(&tables_dev_[k]), sizeof(BatchTables));
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&tables_host_[k]), sizeof(BatchTables));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&counters_dev_[k]), sizeof(BatchCounters));
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&counters_host_[k]), sizeof(BatchCounters));
+    if (e == cudaSuccess) e = cudaMemset(counters_dev_[k], 0, sizeof(BatchCounters));
+    if (e == cudaSuccess) e = cudaMemset(tables_dev_[k], 0, sizeof(BatchTables));
+  }
+  const size_t bin_bytes = sizeof(unsigned int) * 2 * kShadeClasses * kMaxBatchScenes;
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&bins1_), bin_bytes);
+  if (e == cudaSuccess) e = cudaMemset(bins1_, 0, bin_bytes);
   if (e == cudaSuccess) e = paths_.reserve(capacity_, slots_);
-  if (e == cudaSuccess) e = batch_grids(&grids_, 0, capacity_);
+  if (e == cudaSuccess) e = batch_grids(&grids_, 0, half_);
   return e;
+}
+
+// The path state of one half of the pool: every per-path array from the
+// half's first path, the shadow queue from its first entry. Shadow slots keep
+// the whole pool's stride (FrameParams.capacity), so they are offset by the
+// half's first path only.
+PathState BatchEngine::slot_state(int slot) const {
+  PathState ps = paths_.state();
+  if (slot == 0) return ps;
+  const size_t off = static_cast<size_t>(half_);
+  ps.ray_o += off;
+  ps.ray_d += off;
+  ps.hit += off;
+  ps.thr += off;
+  ps.rad += off;
+  ps.med += off;
+  ps.rng += off;
+  ps.flags += off;
+  ps.smask += off;
+  ps.sample += off;
+  ps.slots += off;
+  ps.queue[0] += off;
+  ps.queue[1] += off;
+  ps.binned += off;
+  ps.cls += off;
+  ps.shadow_queue += 3 * off * static_cast<size_t>(paths_.slots());
+  ps.seg += off;
+  ps.bins = bins1_;
+  return ps;
 }
 
 bool BatchEngine::scene_busy(int slot) const {
@@ -129,9 +169,11 @@ cudaError_t BatchEngine::set_scene(int slot, const DScene& scene, int lights) {
   if (slot < 0 || slot >= kMaxBatchScenes || lights < 0) return cudaErrorInvalidValue;
   if (scene_busy(slot)) return cudaErrorNotReady;
   cudaSetDevice(device_);
-  // Chunks in flight keep the old graph and path state: wait for them.
-  cudaError_t e = cudaStreamSynchronize(stream_);
-  if (e != cudaSuccess) return e;
+  // Chunks in flight keep the old graphs and path state: wait for them.
+  for (cudaStream_t st : stream_) {
+    const cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+  }
   scenes_[slot] = scene;
   lights_[slot] = lights;
   scene_set_[slot] = true;
@@ -140,53 +182,64 @@ cudaError_t BatchEngine::set_scene(int slot, const DScene& scene, int lights) {
   for (int i = 0; i < nscenes_; i++)
     if (scene_set_[i]) slots = std::max(slots, lights_[i] + 1);
   if (slots > paths_.slots()) {
-    e = paths_.reserve(capacity_, slots);
+    const cudaError_t e = paths_.reserve(capacity_, slots);
     if (e != cudaSuccess) return e;
   }
   slots_ = std::max(slots_, slots);
-  graph_valid_ = false;
+  graph_valid_[0] = graph_valid_[1] = false;
   return cudaSuccess;
 }
 
 cudaError_t BatchEngine::set_variant(int variant) {
   if (variant == grids_.variant) return cudaSuccess;
   cudaSetDevice(device_);
-  cudaError_t e = cudaStreamSynchronize(stream_);
-  if (e == cudaSuccess) e = batch_grids(&grids_, variant, capacity_);
-  graph_valid_ = false;
+  cudaError_t e = cudaSuccess;
+  for (cudaStream_t st : stream_)
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = batch_grids(&grids_, variant, half_);
+  graph_valid_[0] = graph_valid_[1] = false;
   return e;
 }
 
-void BatchEngine::destroy_graph() {
-  if (exec_) cudaGraphExecDestroy(exec_);
-  if (graph_) cudaGraphDestroy(graph_);
-  exec_ = nullptr;
-  graph_ = nullptr;
-  graph_valid_ = false;
+void BatchEngine::destroy_graphs() {
+  for (int k = 0; k < kSlots; k++) {
+    if (exec_[k]) cudaGraphExecDestroy(exec_[k]);
+    if (graph_[k]) cudaGraphDestroy(graph_[k]);
+    exec_[k] = nullptr;
+    graph_[k] = nullptr;
+    graph_valid_[k] = false;
+  }
 }
 
-// One graph per scene set: raygen, a while node around the bounce iteration
-// (its last kernel sets the condition), then accumulate. Every kernel reads
-// the chunk from tables_dev_, so the graph is reused by every chunk.
-cudaError_t BatchEngine::ensure_graph() {
-  if (!use_graph_ || graph_valid_) return cudaSuccess;
-  destroy_graph();
-  const PathState ps = paths_.state();
+// One graph per half of the pool and scene set: raygen, then a while node
+// around the bounce iteration (its last kernel sets the condition). Every
+// kernel reads the chunk from the half's device tables, so the graph is
+// reused by every chunk of that half. Accumulation runs after the graph, in
+// chunk order (launch()).
+cudaError_t BatchEngine::ensure_graph(int slot) {
+  if (!use_graph_ || graph_valid_[slot]) return cudaSuccess;
+  if (exec_[slot]) cudaGraphExecDestroy(exec_[slot]);
+  if (graph_[slot]) cudaGraphDestroy(graph_[slot]);
+  exec_[slot] = nullptr;
+  graph_[slot] = nullptr;
+  const PathState ps = slot_state(slot);
+  cudaStream_t st = stream_[slot];
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
-  cudaError_t e = cudaGraphCreate(&graph_, 0);
-  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(stream_, graph_, nullptr, nullptr, 0, mode);
+  cudaGraph_t& graph = graph_[slot];
+  cudaError_t e = cudaGraphCreate(&graph, 0);
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0, mode);
   if (e != cudaSuccess) return e;
-  cudaError_t le = launch_batch_raygen(tables_dev_, ps, grids_, stream_);
-  e = cudaStreamEndCapture(stream_, &graph_);
+  cudaError_t le = launch_batch_raygen(tables_dev_[slot], ps, grids_, st);
+  e = cudaStreamEndCapture(st, &graph);
   if (e == cudaSuccess) e = le;
   if (e != cudaSuccess) return e;
   size_t n = 0;
-  e = cudaGraphGetNodes(graph_, nullptr, &n);
+  e = cudaGraphGetNodes(graph, nullptr, &n);
   if (e != cudaSuccess) return e;
   std::vector<cudaGraphNode_t> roots(n);
-  if (n > 0) e = cudaGraphGetNodes(graph_, roots.data(), &n);
+  if (n > 0) e = cudaGraphGetNodes(graph, roots.data(), &n);
   cudaGraphConditionalHandle handle = 0;
-  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, graph_, 1, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
   if (e != cudaSuccess) return e;
   cudaGraphNodeParams p{};
   p.type = cudaGraphNodeTypeConditional;
@@ -194,22 +247,17 @@ cudaError_t BatchEngine::ensure_graph() {
   p.conditional.type = cudaGraphCondTypeWhile;
   p.conditional.size = 1;
   cudaGraphNode_t loop = nullptr;
-  e = cudaGraphAddNode(&loop, graph_, roots.data(), n, &p);
+  e = cudaGraphAddNode(&loop, graph, roots.data(), n, &p);
   if (e != cudaSuccess) return e;
   cudaGraph_t body = p.conditional.phGraph_out[0];
-  e = cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, mode);
+  e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, mode);
   if (e != cudaSuccess) return e;
-  le = launch_batch_iteration(scenes_, nscenes_, tables_dev_, ps, paths_.capacity(), paths_.slots(), counters_dev_,
-                              grids_, true, handle, stream_, &lanes_);
-  e = cudaStreamEndCapture(stream_, &body);
+  le = launch_batch_iteration(scenes_, nscenes_, tables_dev_[slot], ps, paths_.capacity(), paths_.slots(),
+                              counters_dev_[slot], grids_, true, handle, st, &lanes_);
+  e = cudaStreamEndCapture(st, &body);
   if (e == cudaSuccess) e = le;
-  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(stream_, graph_, &loop, nullptr, 1, mode);
-  if (e != cudaSuccess) return e;
-  le = launch_batch_accumulate(tables_dev_, ps, grids_, stream_);
-  e = cudaStreamEndCapture(stream_, &graph_);
-  if (e == cudaSuccess) e = le;
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec_, graph_, 0);
-  if (e == cudaSuccess) graph_valid_ = true;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec_[slot], graph, 0);
+  if (e == cudaSuccess) graph_valid_[slot] = true;
   return e;
 }
 
@@ -256,7 +304,7 @@ bool BatchEngine::admit(Request& r) {
   if (!p) return false;
   r.sum = static_cast<float4*>(p);
   r.image = static_cast<uint8_t*>(p) + sum_bytes;
-  cudaMemsetAsync(r.sum, 0, pix * sizeof(float4), stream_);
+  // No clearing: a pixel's first pass starts its sum from zero (k_batch_accumulate).
   r.admitted = true;
   return true;
 }
@@ -267,7 +315,7 @@ bool BatchEngine::admit(Request& r) {
 // else a pixel range of the next pass that fills the room.
 constexpr int kMinFragment = 1 << 16;
 void BatchEngine::plan(Chunk& c) {
-  long long room = chunk_paths_ > 0 ? std::min(chunk_paths_, capacity_) : capacity_;
+  long long room = chunk_paths_ > 0 ? std::min(chunk_paths_, half_) : half_;
   for (auto& rp : requests_) {
     Request& r = *rp;
     if (r.admitted || r.cancelled) continue;
@@ -286,9 +334,9 @@ void BatchEngine::plan(Chunk& c) {
     if (!active(r) || r.preview != 1 || static_cast<int>(c.segs.size()) >= kMaxSegments) continue;
     const int b = r.d.preview_block;
     const long long blocks = static_cast<long long>((r.d.fp.width + b - 1) / b) * ((r.d.fp.height + b - 1) / b);
-    // A preview larger than the chunk size (never than the pool: submission
-    // checks) goes alone into an empty chunk.
-    if (blocks > room && !(c.segs.empty() && blocks <= capacity_)) continue;
+    // A preview larger than the chunk size (never than half the pool:
+    // submission checks) goes alone into an empty chunk.
+    if (blocks > room && !(c.segs.empty() && blocks <= half_)) continue;
     take(r, 1, 0, 1, 0, static_cast<int>(blocks));
     r.preview = 2;
   }
@@ -325,7 +373,9 @@ void BatchEngine::plan(Chunk& c) {
 }
 
 cudaError_t BatchEngine::launch(Chunk& c) {
-  BatchTables* T = tables_host_[c.slot];
+  const int k = c.slot;
+  cudaStream_t st = stream_[k];
+  BatchTables* T = tables_host_[k];
   const int nseg = static_cast<int>(c.segs.size());
   T->segments = nseg;
   T->iteration = 0;
@@ -378,32 +428,36 @@ cudaError_t BatchEngine::launch(Chunk& c) {
   if (!c.start) e = cudaEventCreate(&c.start);
   if (e == cudaSuccess && !c.done) e = cudaEventCreate(&c.done);
   if (e == cudaSuccess && !c.copied) e = cudaEventCreateWithFlags(&c.copied, cudaEventDisableTiming);
-  if (e == cudaSuccess) e = ensure_graph();
-  if (e == cudaSuccess) e = cudaEventRecord(c.start, stream_);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(tables_dev_, T, bytes, cudaMemcpyHostToDevice, stream_);
-  // An image of this chunk's requests may still be on its way to the host
-  // from the chunk before: the kernels below rewrite it, so wait for the copy.
-  bool wait_copy = false;
-  for (const SegmentPlan& s : c.segs) wait_copy = wait_copy || s.r->copying > 0;
-  if (e == cudaSuccess && wait_copy && copy_pending_) e = cudaStreamWaitEvent(stream_, last_copy_, 0);
+  if (e == cudaSuccess) e = ensure_graph(k);
+  if (e == cudaSuccess) e = cudaEventRecord(c.start, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tables_dev_[k], T, bytes, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return e;
-  const PathState ps = paths_.state();
+  const PathState ps = slot_state(k);
   if (use_graph_) {
-    e = cudaGraphLaunch(exec_, stream_);
+    e = cudaGraphLaunch(exec_[k], st);
     totals_.graph_launches++;
   } else {
-    e = launch_batch_raygen(tables_dev_, ps, grids_, stream_);
+    e = launch_batch_raygen(tables_dev_[k], ps, grids_, st);
     for (int it = 0; e == cudaSuccess && it < T->max_iterations; it++) {
-      e = launch_batch_iteration(scenes_, nscenes_, tables_dev_, ps, paths_.capacity(), paths_.slots(), counters_dev_,
-                                 grids_, false, 0, stream_);
+      e = launch_batch_iteration(scenes_, nscenes_, tables_dev_[k], ps, paths_.capacity(), paths_.slots(),
+                                 counters_dev_[k], grids_, false, 0, st);
       if (e == cudaSuccess)
-        e = cudaMemcpyAsync(counters_host_, counters_dev_, sizeof(BatchCounters), cudaMemcpyDeviceToHost, stream_);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
-      if (e == cudaSuccess && !counters_host_->more) break;
+        e = cudaMemcpyAsync(counters_host_[k], counters_dev_[k], sizeof(BatchCounters), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e == cudaSuccess && !counters_host_[k]->more) break;
     }
-    if (e == cudaSuccess) e = launch_batch_accumulate(tables_dev_, ps, grids_, stream_);
   }
-  if (e == cudaSuccess) e = cudaEventRecord(c.done, stream_);
+  // Accumulation in chunk order: after the previous chunk's (the other half
+  // may still be tracing it), and after any copy to the host of an image this
+  // chunk rewrites.
+  bool wait_copy = false;
+  for (const SegmentPlan& s : c.segs) wait_copy = wait_copy || s.r->copying > 0;
+  if (e == cudaSuccess && wait_copy && copy_pending_) e = cudaStreamWaitEvent(st, last_copy_, 0);
+  if (e == cudaSuccess && accumulated_pending_) e = cudaStreamWaitEvent(st, accumulated_, 0);
+  if (e == cudaSuccess) e = launch_batch_accumulate(tables_dev_[k], ps, grids_, st);
+  if (e == cudaSuccess) e = cudaEventRecord(accumulated_, st);
+  if (e == cudaSuccess) accumulated_pending_ = true;
+  if (e == cudaSuccess) e = cudaEventRecord(c.done, st);
   if (e != cudaSuccess) return e;
   totals_.chunks++;
   // Images a request's client is waiting for: its preview, the image after
@@ -434,13 +488,21 @@ cudaError_t BatchEngine::finish(Chunk& c, std::vector<BatchEvent>& events) {
   cudaError_t e = cudaEventSynchronize(c.done);
   if (e == cudaSuccess && c.copies) e = cudaEventSynchronize(c.copied);
   if (e != cudaSuccess) return e;
+  // Device time once: the part of this chunk after the chunk finished
+  // before it (the two halves overlap).
   float ms = 0;
-  if (cudaEventElapsedTime(&ms, c.start, c.done) == cudaSuccess) totals_.gpu_ms += ms;
-  e = cudaMemcpy(counters_host_, counters_dev_, sizeof(BatchCounters), cudaMemcpyDeviceToHost);
+  if (cudaEventElapsedTime(&ms, c.start, c.done) == cudaSuccess) {
+    float since = 0;
+    if (held_done_ && cudaEventElapsedTime(&since, held_done_, c.done) == cudaSuccess) ms = std::min(ms, std::max(since, 0.0f));
+    totals_.gpu_ms += ms;
+  }
+  const int k = c.slot;
+  e = cudaMemcpy(counters_host_[k], counters_dev_[k], sizeof(BatchCounters), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return e;
-  totals_.closest = counters_host_->closest;
-  totals_.any = counters_host_->any;
-  totals_.status |= counters_host_->status;
+  slot_totals_[k] = *counters_host_[k];
+  totals_.closest = slot_totals_[0].closest + slot_totals_[1].closest;
+  totals_.any = slot_totals_[0].any + slot_totals_[1].any;
+  totals_.status |= slot_totals_[k].status;
   for (size_t j = 0; j < c.segs.size(); j++) {
     const SegmentPlan& s = c.segs[j];
     Request& r = *s.r;
@@ -494,7 +556,8 @@ cudaError_t BatchEngine::step(std::vector<BatchEvent>& events, bool* idle, bool*
     e = finish(inflight_.front(), events);
     Chunk& done = inflight_.front();
     if (done.start) cudaEventDestroy(done.start);
-    if (done.done) cudaEventDestroy(done.done);
+    if (held_done_) cudaEventDestroy(held_done_);
+    held_done_ = done.done;  // the next chunk's device time counts from here
     if (done.copied) cudaEventDestroy(done.copied);
     inflight_.pop_front();
     if (e != cudaSuccess) return e;

@@ -72,9 +72,10 @@ class BatchEngine {
   BatchEngine(const BatchEngine&) = delete;
   BatchEngine& operator=(const BatchEngine&) = delete;
 
-  // `capacity`: paths per chunk; `arena_bytes`: budget for the requests'
-  // sums and images; `use_graph`: run each chunk's bounce loop as a CUDA
-  // graph with a while node (else a host-driven loop, one sync per bounce).
+  // `capacity`: paths in the pool, which two chunks share half and half;
+  // `arena_bytes`: budget for the requests' sums and images; `use_graph`: run
+  // each chunk's bounce loop as a CUDA graph with a while node (else a
+  // host-driven loop, one sync per bounce).
   cudaError_t init(int device, int capacity, size_t arena_bytes, bool use_graph);
   // Puts a scene into `slot` (< kMaxBatchScenes) with `lights` lights. Fails
   // while requests on the slot are unfinished.
@@ -95,18 +96,26 @@ class BatchEngine {
   cudaError_t step(std::vector<BatchEvent>& events, bool* idle, bool* progressed = nullptr);
   BatchTotals totals() const { return totals_; }
   int capacity() const { return capacity_; }
+  // The most paths one chunk holds: half the pool (two chunks run at once).
+  int max_chunk_paths() const { return half_; }
   size_t path_bytes() const { return paths_.bytes(); }
   const DeviceArena& arena() const { return arena_; }
-  cudaStream_t stream() const { return stream_; }
-  // Limits a chunk to `paths` paths (<= capacity): smaller chunks bound the
-  // latency of a new request's preview under load.
+  // Limits a chunk to `paths` paths (<= max_chunk_paths): smaller chunks bound
+  // the latency of a new request's preview under load.
   void set_chunk_paths(int paths) { chunk_paths_ = paths; }
   // Traversal kernel variant (traversal_variant_info); waits for chunks in
-  // flight and rebuilds the graph on the next launch.
+  // flight and rebuilds the graphs on the next launch.
   cudaError_t set_variant(int variant);
   int variant() const { return grids_.variant; }
 
  private:
+  // Two chunks run at once, each in its own half of the path pool with its
+  // own stream, tables, counters, shading-order bins and graph, so one
+  // chunk's bounce tails (the last, slowest paths of each stage) overlap the
+  // other's work. Accumulation stays in chunk order (an event chain), so a
+  // request's pixels still add their passes in pass order.
+  static constexpr int kSlots = 2;
+
   struct Request {
     long long id;
     BatchRequestDesc d;
@@ -129,7 +138,7 @@ class BatchEngine {
     int pass0, passes, pix0, npix, done_after;
   };
   struct Chunk {
-    int slot;  // pinned table buffer
+    int slot;  // half of the pool, stream, tables and graph
     std::vector<SegmentPlan> segs;
     cudaEvent_t start = nullptr, done = nullptr, copied = nullptr;
     bool copies = false;
@@ -138,8 +147,9 @@ class BatchEngine {
     std::vector<int> passes_done;
   };
 
-  cudaError_t ensure_graph();
-  void destroy_graph();
+  PathState slot_state(int slot) const;
+  cudaError_t ensure_graph(int slot);
+  void destroy_graphs();
   bool admit(Request& r);
   void plan(Chunk& c);
   cudaError_t launch(Chunk& c);
@@ -147,32 +157,40 @@ class BatchEngine {
   void release(Request& r);
 
   int device_ = 0;
-  int capacity_ = 0, chunk_paths_ = 0;
+  int capacity_ = 0, half_ = 0, chunk_paths_ = 0;
   int slots_ = 1;
   bool use_graph_ = true;
-  cudaStream_t stream_ = nullptr, copy_stream_ = nullptr;
+  cudaStream_t stream_[kSlots] = {};
+  cudaStream_t copy_stream_ = nullptr;
   SceneLanes lanes_{};  // per-scene branches of the captured bounce iteration
   PathBuffers paths_;
+  unsigned int* bins1_ = nullptr;  // slot 1's shading-order bins (slot 0 uses the pool's)
   DeviceArena arena_;
-  BatchTables* tables_dev_ = nullptr;
-  BatchTables* tables_host_[2] = {nullptr, nullptr};
-  BatchCounters* counters_dev_ = nullptr;
-  BatchCounters* counters_host_ = nullptr;
+  BatchTables* tables_dev_[kSlots] = {};
+  BatchTables* tables_host_[kSlots] = {};
+  BatchCounters* counters_dev_[kSlots] = {};
+  BatchCounters* counters_host_[kSlots] = {};
+  BatchCounters slot_totals_[kSlots] = {};  // each slot's counters after its last finished chunk
   BatchGrids grids_{};
   DScene scenes_[kMaxBatchScenes]{};
   int lights_[kMaxBatchScenes]{};
   bool scene_set_[kMaxBatchScenes]{};
   int nscenes_ = 0;
-  cudaGraph_t graph_ = nullptr;
-  cudaGraphExec_t exec_ = nullptr;
-  bool graph_valid_ = false;
+  cudaGraph_t graph_[kSlots] = {};
+  cudaGraphExec_t exec_[kSlots] = {};
+  bool graph_valid_[kSlots] = {};
   long long next_id_ = 1;
   std::deque<std::unique_ptr<Request>> requests_;  // submission order
   std::deque<Chunk> inflight_;
-  // Copy-stream event of the last chunk that copied images to the host: the
-  // next chunk waits for it, so no kernel rewrites an image being copied.
+  // Copy-stream event of the last chunk that copied images to the host: a
+  // chunk's accumulation waits for it before rewriting an image being copied.
   cudaEvent_t last_copy_ = nullptr;
   bool copy_pending_ = false;
+  // Recorded after each chunk's accumulation; the next chunk's waits for it.
+  cudaEvent_t accumulated_ = nullptr;
+  bool accumulated_pending_ = false;
+  // Done event of the chunk finished last, kept to count overlapped time once.
+  cudaEvent_t held_done_ = nullptr;
   int next_slot_ = 0;
   BatchTotals totals_;
 };

@@ -1319,8 +1319,8 @@ int64_t submit_request(mcrt_batch* b, const mcrt_request* r) {
   if (d.preview_block > 1) {
     const long long blocks = static_cast<long long>((r->width + d.preview_block - 1) / d.preview_block) *
                              ((r->height + d.preview_block - 1) / d.preview_block);
-    if (blocks > b->engine.capacity())
-      fail(MCRT_ERR_LIMIT, "the block preview needs more paths than the batch's path pool holds");
+    if (blocks > b->engine.max_chunk_paths())
+      fail(MCRT_ERR_LIMIT, "the block preview needs more paths than one chunk of the batch's pool holds (half the pool)");
   }
   d.scene = scene_slot(b, r);
   const long long id = b->engine.submit(d, r->image, r->preview_image, r->progress_image);
@@ -1339,7 +1339,7 @@ int32_t mcrt_batch_create(int32_t device, int32_t capacity, int64_t arena_bytes,
     int c = 0;
     cuda_check(cudaGetDeviceCount(&c), "cudaGetDeviceCount");
     if (device < 0 || device >= c) fail(MCRT_ERR_INVALID, "no such CUDA device");
-    if (capacity < 1) fail(MCRT_ERR_INVALID, "capacity must be positive");
+    if (capacity < 2) fail(MCRT_ERR_INVALID, "capacity must be at least 2 (two chunks share the pool)");
     if (arena_bytes < 4096) fail(MCRT_ERR_INVALID, "memory budget too small");
     std::unique_ptr<mcrt_batch> b(new mcrt_batch());
     b->device = device;

@@ -180,7 +180,6 @@ __global__ void __launch_bounds__(B, 1280 / B) k_extend(DScene sc, PathState ps,
 // material of one model, transmissive or not. Shading the queue in that
 // class order gives each warp lanes that take the same branches (and run
 // the same code) instead of a mix; results do not depend on queue order.
-constexpr int kShadeClasses = 16;
 
 MCRT_D int shade_class(const DScene& sc, const PathState& ps, int pid) {
   const unsigned word = __float_as_uint(__ldg(reinterpret_cast<const float*>(ps.hit + pid) + 3));
@@ -1636,7 +1635,9 @@ __global__ void __launch_bounds__(256) k_batch_accumulate(const BatchTables* __r
       continue;
     }
     const int gi = fp.pix0 + i;
-    float4 sm = o.sum[gi];
+    // A segment starting at pass 0 starts the pixel's running sum (request
+    // buffers are not cleared when they are taken from the arena).
+    float4 sm = fp.pass0 == 0 ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : o.sum[gi];
     double r = 0, g = 0, b = 0, a = 0;
     for (int jj = 0; jj < o.passes; jj++) {
       const float4 x = samples[static_cast<size_t>(jj) * fp.npix + i];

@@ -139,6 +139,10 @@ cudaError_t primary_hits(const DScene& scene, FrameParams fp, PathBuffers& buffe
 // [base, base + paths), and its queue entries and shadow rays use the
 // matching ranges of the queues, so every stage runs once per scene.
 constexpr int kMaxBatchScenes = 8;
+// Shading classes of the hit-class sort: a miss, or a material model,
+// transmissive or not (render.cu shade_class). The sort's bins hold two
+// counters per class and scene.
+constexpr int kShadeClasses = 16;
 constexpr int kMaxSegments = 256;
 constexpr unsigned kStatusIterationLimit = 16u;  // a chunk still had paths after max_iterations
 

@@ -153,11 +153,11 @@ def test_cancelled_requests_return_their_memory(two_scenes):
 
 
 def test_progress_events_report_completed_passes(two_scenes):
-    # 64 x 48 = 3072 pixels; a 6144-path chunk holds two passes, so a 6-sample render
-    # reports progress at 2 and 4 passes, then done at 6.
+    # 64 x 48 = 3072 pixels; a 6144-path chunk (half of the pool) holds two passes, so a
+    # 6-sample render reports progress at 2 and 4 passes, then done at 6.
     s_scene, s_cam, s_st = two_scenes[0]
     w, h = 64, 48
-    renderer = BatchRenderer(capacity=2 * w * h, memory_budget=64 << 20)
+    renderer = BatchRenderer(capacity=4 * w * h, memory_budget=64 << 20)
     try:
         rid = renderer.submit(RenderRequest(s_scene, s_cam, w, h, s_st, 6, progress=True))
         seen, frames = [], []
