@@ -374,7 +374,8 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                                           f"{base['seconds']:.1f} s) of the same workload on the oracle, a C++ "
                                           f"restatement of the reference's TypeScript path (no Node.js here)"}
     if world == 1 and not args.no_large:
-        line["large"] = run_large(local, args.large_count, args.large_frames, tune=not args.no_tune)
+        line["large"] = run_large(local, args.large_count, args.large_frames, tune=not args.no_tune,
+                                  capacity=args.capacity, size=args.large_size)
     if world == 1 and not (args.no_batch and args.no_serve):
         # The batched and served forms of the same path, beside the plain number.
         from meercadraytracer_b200 import scenes as SC
@@ -390,7 +391,8 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
             extra["big"] = _compile(big.scene, builder=ex.compile_sink)
             extra["soup"] = _compile(SC.soup_scene().scene, builder=ex.compile_sink)
             t_scenes = time.perf_counter() - t0
-            line["served"] = run_served(extra, local, args.serve_seconds, args.serve_capacity, args.serve_chunk)
+            line["served"] = run_served(extra, local, args.serve_seconds, args.serve_capacity, args.serve_chunk,
+                                        args.serve_target_ms)
             line["served"]["scene_build_s"] = round(t_scenes, 2)
     print(json.dumps(line), flush=True)
     if dist:
@@ -508,7 +510,8 @@ def run_batched(compiled: Dict[str, Any], device: int, capacity: int, seed: int 
 
 
 # ------------------------------------------------------------- serving loop
-def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: int, chunk: int) -> Dict[str, Any]:
+def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: int, chunk: int,
+               target_ms: float = 18.0) -> Dict[str, Any]:
     """The serving loop: 8 clients, two per resident scene, orbiting at 30 deg/s with Poisson
     camera moves (mean 100 ms); each move restarts the client's request: an 8x8 block preview,
     then 64 spp at 1280x720, GI on, 4 bounces. After `seconds` the moves stop and each
@@ -525,8 +528,9 @@ def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: 
     try:
         for n in names:
             server.add_scene(n, compiled[n])
-        # The autotuner sizes chunks so one takes about 12 ms on the slowest scene (a new
-        # request's preview waits for at most the chunks in flight), unless given.
+        # The autotuner sizes chunks so one takes about `target_ms` on the slowest scene (a
+        # new request's preview waits for at most the chunks in flight), unless given.
+        # 18 ms: the largest chunk (half the pool) with p99 time-to-preview near 30 ms.
         from meercadraytracer_b200 import autotune
         from meercadraytracer_b200.batch import RenderRequest
         from meercadraytracer_b200.compile import compile_camera
@@ -536,7 +540,7 @@ def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: 
             probes = [RenderRequest(compiled[c.scene], compile_camera(orbit_camera(c.radius, c.height, c.phase,
                                                                                    aspect=16 / 9)),
                                     1280, 720, settings, 1) for c in clients[: len(names)]]
-            chunk = autotune.tune_serving_chunk(server.batch, probes, target_ms=12.0).chunk
+            chunk = autotune.tune_serving_chunk(server.batch, probes, target_ms=target_ms).chunk
         # Warm-up: one short request per scene (graph instantiation, first-touch).
         simulate_clients(server, clients[: len(names)], {n: settings for n in names}, duration=0.2, width=320,
                          height=180, samples=2, seed=1)
@@ -552,7 +556,8 @@ def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: 
 
 
 # ------------------------------------------------------ per-frame rebuild
-def run_large(device: int, count: int, frames: int, bins: int = 32, tune: bool = True) -> Dict[str, Any]:
+def run_large(device: int, count: int, frames: int, bins: int = 32, tune: bool = True, capacity: int = 0,
+              size: int = 0) -> Dict[str, Any]:
     """The large workload: `count` icospheres (20,480 triangles each) under rigid transforms
     re-drawn every frame; each frame compiles the instances on the GPU (flatten, binned-SAH
     BVH with `bins` bins, reorder, tangents) and renders 2048 x 2048 at 16 spp, GI on,
@@ -565,10 +570,12 @@ def run_large(device: int, count: int, frames: int, bins: int = 32, tune: bool =
     from meercadraytracer_b200.executors import GpuExecutor
     from meercadraytracer_b200.raytrace import as_options, output_srgb, sample_count, trace_settings
 
-    L = SC.large_scene(count=count)
+    L = SC.large_scene(count=count, **({"width": size, "height": size} if size else {}))
     o = as_options(L.options)
     st, spp, srgb = trace_settings(o), sample_count(o), output_srgb(o)
     ex = GpuExecutor(device)
+    if capacity:
+        ex.set_capacity(capacity)
     try:
         free0, total_mem = torch.cuda.mem_get_info(device)
         ex.upload_meshes([L.mesh])
@@ -657,7 +664,11 @@ def main() -> None:
     ap.add_argument("--batch-capacity", type=int, default=1 << 24, help="path pool of the batch engine")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the served client simulation")
     ap.add_argument("--serve-capacity", type=int, default=1 << 22, help="path pool of the serving loop")
-    ap.add_argument("--serve-chunk", type=int, default=0, help="paths per chunk in the serving loop (0: pool)")
+    ap.add_argument("--serve-chunk", type=int, default=0, help="paths per chunk in the serving loop (0: autotuned)")
+    ap.add_argument("--serve-target-ms", type=float, default=18.0,
+                    help="serving chunk autotune: device time of one chunk on the slowest resident scene")
+    ap.add_argument("--large-size", type=int, default=0, help="image side of the per-frame rebuild workload "
+                                                              "(0: 2048; smaller for profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be at least 3")
@@ -666,7 +677,8 @@ def main() -> None:
         run_reference(args, rank)
     elif args.large_only:
         if rank == 0:
-            print(json.dumps({"large": run_large(local, args.large_count, args.large_frames, tune=not args.no_tune)}), flush=True)
+            print(json.dumps({"large": run_large(local, args.large_count, args.large_frames, tune=not args.no_tune,
+                                                 capacity=args.capacity, size=args.large_size)}), flush=True)
     else:
         run_ours(args, rank, world, local)
 
