@@ -511,7 +511,7 @@ def run_batched(compiled: Dict[str, Any], device: int, capacity: int, seed: int 
 
 # ------------------------------------------------------------- serving loop
 def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: int, chunk: int,
-               target_ms: float = 18.0) -> Dict[str, Any]:
+               target_ms: float = 24.0) -> Dict[str, Any]:
     """The serving loop: 8 clients, two per resident scene, orbiting at 30 deg/s with Poisson
     camera moves (mean 100 ms); each move restarts the client's request: an 8x8 block preview,
     then 64 spp at 1280x720, GI on, 4 bounces. After `seconds` the moves stop and each
@@ -530,7 +530,8 @@ def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: 
             server.add_scene(n, compiled[n])
         # The autotuner sizes chunks so one takes about `target_ms` on the slowest scene (a
         # new request's preview waits for at most the chunks in flight), unless given.
-        # 18 ms: the largest chunk (half the pool) with p99 time-to-preview near 30 ms.
+        # 24 ms with an 8M-path pool: p99 time-to-preview near 37 ms (target 50), and the
+        # most rays per second of the settings measured (12 / 18 / 24 ms, 4M / 8M paths).
         from meercadraytracer_b200 import autotune
         from meercadraytracer_b200.batch import RenderRequest
         from meercadraytracer_b200.compile import compile_camera
@@ -661,11 +662,13 @@ def main() -> None:
     ap.add_argument("--large-only", action="store_true",
                     help="run only the per-frame rebuild workload and print its record (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop run")
-    ap.add_argument("--batch-capacity", type=int, default=1 << 24, help="path pool of the batch engine")
+    ap.add_argument("--batch-capacity", type=int, default=1 << 25,
+                    help="path pool of the batch engine (two chunks of half of it run at once)")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the served client simulation")
-    ap.add_argument("--serve-capacity", type=int, default=1 << 22, help="path pool of the serving loop")
+    ap.add_argument("--serve-capacity", type=int, default=1 << 23,
+                    help="path pool of the serving loop (two chunks of half of it run at once)")
     ap.add_argument("--serve-chunk", type=int, default=0, help="paths per chunk in the serving loop (0: autotuned)")
-    ap.add_argument("--serve-target-ms", type=float, default=18.0,
+    ap.add_argument("--serve-target-ms", type=float, default=24.0,
                     help="serving chunk autotune: device time of one chunk on the slowest resident scene")
     ap.add_argument("--large-size", type=int, default=0, help="image side of the per-frame rebuild workload "
                                                               "(0: 2048; smaller for profiling runs)")
