@@ -66,8 +66,15 @@ MCRT_D void walk(const DScene& sc, Q& q, int n, unsigned* counter, unsigned& sta
 // ---------------------------------------------------------------- mapping
 MCRT_D void path_pixel(const FrameParams& fp, int pid, int& px, int& py, int& pass) {
   const int k = pid - fp.path_base;
-  int j = k / fp.npix;
-  int i = fp.pix0 + (k - j * fp.npix);
+  int i, j;
+  if (fp.npass > 0) {
+    i = k / fp.npass;
+    j = k - i * fp.npass;
+  } else {
+    j = k / fp.npix;
+    i = k - j * fp.npix;
+  }
+  i += fp.pix0;
   pass = fp.pass0 + j;
   if (fp.mode == 1) {
     px = fp.list_x[i];
@@ -953,8 +960,9 @@ MCRT_D uchar4 encode_rgba(double r, double g, double b, double a, double scale, 
   return o;
 }
 
-// writeTile, progressive.ts:295-310, over the passes of one chunk in order.
-// The running sum is Float32; the encode reads the last pass's sum unrounded,
+// writeTile, progressive.ts:295-310, over the passes of one chunk in order
+// (the plain wavefront runs a chunk's paths pixel-major, so pixel i's samples
+// are the `passes` consecutive ones from i * passes). The running sum is Float32; the encode reads the last pass's sum unrounded,
 // as `r = sum[d] = sum[d] + r` does, in double.
 __global__ void __launch_bounds__(256) k_accumulate(const float4* __restrict__ samples, int npix, int passes,
                                                     float4* __restrict__ sum, int total_passes, int last_chunk,
@@ -965,7 +973,7 @@ __global__ void __launch_bounds__(256) k_accumulate(const float4* __restrict__ s
   float4 s = sum[gi];
   double r = 0, g = 0, b = 0, a = 0;
   for (int j = 0; j < passes; j++) {
-    const float4 x = samples[static_cast<size_t>(j) * npix + i];
+    const float4 x = samples[static_cast<size_t>(i) * passes + j];
     r = static_cast<double>(s.x) + x.x;
     g = static_cast<double>(s.y) + x.y;
     b = static_cast<double>(s.z) + x.z;
@@ -1300,6 +1308,7 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
     int n = np * npix;
     FrameParams f = fp;
     f.pass0 = fp.pass0 + first;
+    f.npass = np;
     tm.start();
     k_raygen<<<blocks_for(n, kBlock), kBlock, 0, stream>>>(f, ps, n);
     tm.stop(st.ms_raygen, st.n_raygen);

@@ -43,7 +43,9 @@ struct FrameParams {
   int slot_count;  // shadow slots per path: lights + 1
   int capacity;    // path-state capacity
   int path_base;   // path id of this launch series' first path (0 unless batched)
+  int npass;       // > 0: the series' passes, pixel-major (path k: pixel k / npass, pass k % npass); 0: pass-major
 };
+
 
 // Structure-of-arrays path state, indexed by path id.
 struct PathState {
