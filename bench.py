@@ -261,12 +261,13 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
 
     tuned: Dict[str, Any] = {}
     if not args.no_tune:
-        # The autotuner picks the traversal variant and the path pool on the same scene and
-        # image at an eighth of the samples (outside the timed region).
+        # The autotuner picks the traversal variant on the same scene and image at an eighth
+        # of the samples, then the path pool at the full sample count (outside the timed region).
         from meercadraytracer_b200 import autotune
 
         choice = autotune.tune_plain(ex, compiled, cam, st, w, h, max(2, spp // 8),
-                                     capacities=(1 << 22, 1 << 23, 1 << 24) if not args.capacity else (args.capacity,))
+                                     capacities=(1 << 23, 1 << 24, 1 << 25) if not args.capacity else (args.capacity,),
+                                     capacity_samples=spp)
         tuned = {"block": choice.block, "stack": choice.stack, "capacity": choice.capacity,
                  "timings_ms": choice.timings}
     for _ in range(args.warmup):

@@ -92,13 +92,19 @@ def _best(timings: Dict[Any, float]) -> Any:
 
 
 def tune_plain(executor: Any, scene: CompiledScene, camera: CompiledCamera, settings: TraceSettings, width: int,
-               height: int, samples: int, capacities: Sequence[int] = (1 << 22, 1 << 23, 1 << 24),
+               height: int, samples: int, capacities: Sequence[int] = (1 << 23, 1 << 24, 1 << 25),
                variants: Optional[Sequence[Tuple[int, int]]] = None, repeats: int = 2,
-               key: Optional[str] = None, cache_path: Optional[str] = None) -> Choice:
+               key: Optional[str] = None, cache_path: Optional[str] = None,
+               capacity_samples: Optional[int] = None) -> Choice:
     """Tunes an executor for raytraceCompiled on `scene`: each traversal variant is timed on
-    the workload at the largest capacity, then the capacities with the best variant. The
-    executor is left set to the choice. Times are device times of whole renders."""
-    key = key or f"plain|{device_name(executor.device)}|{scene.geometry.triangle_count}|{width}x{height}x{samples}"
+    the workload at the largest capacity, then the capacities with the best variant, at
+    `capacity_samples` samples per pixel (default `samples`): a frame takes every pass of as
+    many pixels as the pool holds, so the pool decides how many chunks a frame of the full
+    sample count takes, which fewer samples do not show. The executor is left set to the
+    choice. Times are device times of whole renders."""
+    cap_spp = capacity_samples or samples
+    key = key or (f"plain|{device_name(executor.device)}|{scene.geometry.triangle_count}|"
+                  f"{width}x{height}x{samples}x{cap_spp}")
     hit = _load(cache_path, key)
     if hit is not None:
         choice = Choice(**hit)
@@ -106,11 +112,11 @@ def tune_plain(executor: Any, scene: CompiledScene, camera: CompiledCamera, sett
         executor.set_capacity(choice.capacity)
         return choice
 
-    def timed() -> float:
+    def timed(spp: int = samples) -> float:
         best = float("inf")
         for _ in range(max(1, repeats)):
             executor.reset_stats()
-            executor.raytrace(scene, camera, width, height, settings, samples, True)
+            executor.raytrace(scene, camera, width, height, settings, spp, True)
             best = min(best, executor.stats()["ms_total"])
         return best
 
@@ -126,7 +132,7 @@ def tune_plain(executor: Any, scene: CompiledScene, camera: CompiledCamera, sett
     tc: Dict[int, float] = {}
     for c in capacities:
         executor.set_capacity(c)
-        tc[c] = timed()
+        tc[c] = timed(cap_spp)
     capacity = _best(tc)
     executor.set_capacity(capacity)
     timings = {f"variant {b}x{s}": round(t, 3) for (b, s), t in tv.items()}

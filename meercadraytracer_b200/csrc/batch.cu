@@ -395,6 +395,7 @@ cudaError_t BatchEngine::launch(Chunk& c) {
     fp.pass0 = s.pass0;
     fp.pix0 = s.pix0;
     fp.npix = s.npix;
+    fp.npass = s.passes;  // pixel-major, as the plain wavefront runs its chunks
     fp.path_base = paths;
     fp.capacity = paths_.capacity();
     fp.slot_count = paths_.slots();

@@ -202,7 +202,7 @@ struct mcrt_executor {
   ShadingGpu sh;
   std::unordered_map<int, std::unique_ptr<TextureGpu>> textures;
   PathBuffers paths;
-  int capacity = 1 << 24;  // paths in flight: 16M, about 9 GB of path state with 5 lights
+  int capacity = 1 << 25;  // paths in flight: 32M, about 17 GB of path state with 5 lights
   int variant = 0;         // traversal kernels' (block, short stack) variant
   int step_limit = 0;      // > 0: a query's step budget (mcrt_set_step_limit)
   bool timed = false;
@@ -350,19 +350,25 @@ cudaError_t tile_chunk(void* p, int, int) {
 }
 
 // Runs `passes` passes over `total` paths per pass in pixel chunks that fit
-// the path state, calling `chunk` after each pass chunk.
+// the path state, calling `chunk` after each pass chunk. A chunk takes every
+// pass of as many pixels as fit, so a warp's paths are passes of one or two
+// pixels (the wavefront runs them pixel-major): near-identical camera rays,
+// and shadow rays from near-identical points. Fewer pixels than passes fit
+// only in a pool smaller than the pass count; the wavefront then splits the
+// passes. Each pixel's passes still reach its sum in pass order.
 void run_frame(mcrt_executor* ex, FrameParams fp, int total, int passes, ChunkCtx& ctx,
                cudaError_t (*chunk)(void*, int, int)) {
   const int cap = reserve_paths(ex, static_cast<long long>(total) * passes);
+  const int span = std::max(1, std::min(total, cap / passes));
   const DScene scene = make_scene(ex);
   cuda_check(cudaEventRecord(ex->ev0, ex->stream), "cudaEventRecord");
   // This call's walk status alone, merged into the running stats afterwards.
   const unsigned earlier = ex->stats.status;
   ex->stats.status = 0;
   cudaError_t e = cudaSuccess;
-  for (int p0 = 0; p0 < total && e == cudaSuccess; p0 += cap) {
+  for (int p0 = 0; p0 < total && e == cudaSuccess; p0 += span) {
     fp.pix0 = p0;
-    fp.npix = std::min(cap, total - p0);
+    fp.npix = std::min(span, total - p0);
     ctx.fp = fp;
     Wavefront wf;
     wf.variant = ex->variant;

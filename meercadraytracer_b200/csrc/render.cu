@@ -1617,8 +1617,9 @@ __global__ void k_batch_advance(BatchTables* t, int nscenes, BatchCounters* bc, 
 }
 
 // writeTile for one segment item: a preview block written straight into the
-// image (no running sum, count 1), or one pixel's passes added in order to the
-// Float32 sum and the average encoded.
+// image (no running sum, count 1), or one pixel's passes (consecutive paths:
+// segments run pixel-major) added in order to the Float32 sum and the average
+// encoded.
 __global__ void __launch_bounds__(256) k_batch_accumulate(const BatchTables* __restrict__ t, PathState ps) {
   __shared__ int base[kMaxSegments + 1];
   const int nseg = t->segments;
@@ -1649,7 +1650,7 @@ __global__ void __launch_bounds__(256) k_batch_accumulate(const BatchTables* __r
     float4 sm = fp.pass0 == 0 ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : o.sum[gi];
     double r = 0, g = 0, b = 0, a = 0;
     for (int jj = 0; jj < o.passes; jj++) {
-      const float4 x = samples[static_cast<size_t>(jj) * fp.npix + i];
+      const float4 x = samples[static_cast<size_t>(i) * o.passes + jj];
       r = static_cast<double>(sm.x) + x.x;
       g = static_cast<double>(sm.y) + x.y;
       b = static_cast<double>(sm.z) + x.z;
