@@ -287,11 +287,15 @@ typedef struct mcrt_request {
   uint8_t* image;           /* host RGBA8, width * height * 4, for the final image; or NULL */
   uint8_t* preview_image;   /* host RGBA8 for the block preview; or NULL */
   uint8_t* progress_image;  /* host RGBA8 refreshed after every chunk that completes a pass short of the
-                               last (ProgressiveFrame with samples < maxSamples); or NULL */
+                               last (ProgressiveFrame with samples < maxSamples); or NULL. Given, the
+                               request's passes are scheduled one pass (or as many whole passes as a
+                               chunk holds) at a time; NULL, in groups of up to 16 passes per pixel,
+                               which trace faster (a warp's rays are passes of one or two pixels) */
 } mcrt_request;
 
 /* PREVIEW: preview_image holds the block preview. PROGRESS: `samples` passes
- * are accumulated (progress_image holds them, if given). DONE: image holds
+ * are accumulated (progress_image holds them, if given); without a
+ * progress_image these come at the ends of pass groups. DONE: image holds
  * the final image. */
 enum { MCRT_EVENT_PREVIEW = 1, MCRT_EVENT_DONE = 2, MCRT_EVENT_PROGRESS = 3 };
 

@@ -44,7 +44,7 @@ class RenderRequest:
     samples: int = 16
     preview_block: int = 0  # > 1: ProgressiveOptions.previewBlock
     srgb: bool = True
-    progress: bool = False  # copy the image to the host after every completed pass
+    progress: bool = False  # copy the image to the host after every completed pass (scheduled pass by pass)
 
 
 class BatchRenderer:

@@ -311,9 +311,14 @@ bool BatchEngine::admit(Request& r) {
 
 // Chooses the chunk's segments: admissions in submission order while the
 // arena has room, previews first, then passes of the admitted requests in
-// submission order, each request at most once: whole passes where they fit,
-// else a pixel range of the next pass that fills the room.
+// submission order, each request at most once: whole passes where a group of
+// kGroupPasses of them (or all that are left) fits, else a pixel range of such
+// a group that fills the room. A segment's paths run pixel-major, so a warp
+// holds passes of one or two pixels: coherent camera and shadow rays. A
+// request that asked for progress images goes by groups of one pass, so its
+// client sees every pass that a chunk completes.
 constexpr int kMinFragment = 1 << 16;
+constexpr int kGroupPasses = 16;
 void BatchEngine::plan(Chunk& c) {
   long long room = chunk_paths_ > 0 ? std::min(chunk_paths_, half_) : half_;
   for (auto& rp : requests_) {
@@ -346,24 +351,30 @@ void BatchEngine::plan(Chunk& c) {
     if (std::find(used.begin(), used.end(), &r) != used.end()) continue;
     if (r.next_pass >= r.d.samples || room <= 0) continue;
     const long long P = r.pixels();
-    if (r.next_pix > 0 || P > room) {
-      // A pass larger than the room left in this chunk, or one already split:
-      // the next pixel range, so chunks run full. A range shorter than
-      // kMinFragment that does not end the pass waits for the next chunk,
-      // unless nothing else is in this one (a chunk smaller than
-      // kMinFragment still makes progress).
-      const int n = static_cast<int>(std::min<long long>(room, P - r.next_pix));
-      if (n <= 0 || (n < kMinFragment && n < P - r.next_pix && !c.segs.empty())) continue;
-      take(r, 0, r.next_pass, 1, r.next_pix, n);
-      r.next_pix += n;
-      if (r.next_pix >= P) {
-        r.next_pix = 0;
-        r.next_pass++;
-      }
-    } else if (P <= room) {
-      const int k = static_cast<int>(std::min<long long>(r.d.samples - r.next_pass, room / P));
+    const int left = r.d.samples - r.next_pass;
+    const int unit = r.host_progress ? 1 : std::min(left, kGroupPasses);
+    if (r.next_pix == 0 && P * unit <= room) {
+      const int k = static_cast<int>(std::min<long long>(left, room / P));
       take(r, 0, r.next_pass, k, 0, static_cast<int>(P));
       r.next_pass += k;
+      continue;
+    }
+    // A pass group larger than the room left in this chunk, or one already
+    // split: its next pixel range, so chunks run full. A group has at most
+    // half the pool's paths per pixel, so one pixel always fits an empty
+    // chunk. A range of fewer than kMinFragment paths that does not end the
+    // group waits for the next chunk, unless nothing else is in this one (a
+    // chunk smaller than kMinFragment still makes progress).
+    if (r.next_pix == 0) r.group = std::min(unit, std::max(half_, 1));
+    const int g = r.group;
+    long long n = std::min<long long>(room / g, P - r.next_pix);
+    if (n <= 0 && c.segs.empty()) n = 1;
+    if (n <= 0 || (n * g < kMinFragment && n < P - r.next_pix && !c.segs.empty())) continue;
+    take(r, 0, r.next_pass, g, r.next_pix, static_cast<int>(n));
+    r.next_pix += static_cast<int>(n);
+    if (r.next_pix >= P) {
+      r.next_pix = 0;
+      r.next_pass += g;
     }
   }
   // Scene-major order: each scene's paths form one range.

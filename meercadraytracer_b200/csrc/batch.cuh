@@ -127,7 +127,8 @@ class BatchEngine {
     bool admitted = false, cancelled = false, finished = false;
     int preview = 0;          // 0 none, 1 to schedule, 2 scheduled
     int next_pass = 0;        // first pass not yet scheduled
-    int next_pix = 0;         // first pixel of next_pass not yet scheduled (split passes)
+    int next_pix = 0;         // first pixel of the pass group at next_pass not yet scheduled
+    int group = 0;            // passes of that group while it is split by pixel range
     int inflight = 0;         // chunks in flight that hold a segment of this request
     int copying = 0;          // chunks in flight copying this request's image to the host
     long long pixels() const { return static_cast<long long>(d.fp.width) * d.fp.height; }
