@@ -182,6 +182,18 @@ __global__ void __launch_bounds__(B, 1280 / B) k_extend(DScene sc, PathState ps,
   if (status) atomicOr(&cnt->status, status);
 }
 
+// The same over a queue of coherent rays (the camera rays), warp by warp
+// (traverse_packet); B / 32 warp stacks of kStackMax entries in shared memory.
+template <int B>
+__global__ void __launch_bounds__(B) k_extend_packet(DScene sc, PathState ps, const int* __restrict__ queue, int n,
+                                                     Counters* cnt) {
+  __shared__ int2 stack[(B / 32) * kStackMax];
+  unsigned status = 0;
+  ExtendQuery q{sc, ps, queue, 0, {}};
+  traverse_packet(sc, q, n, &cnt->fetch, stack + (threadIdx.x >> 5) * kStackMax, status);
+  if (status) atomicOr(&cnt->status, status);
+}
+
 // ------------------------------------------------------- shading order
 // The shading step branches on what a path hit: nothing (background), or a
 // material of one model, transmissive or not. Shading the queue in that
@@ -1323,9 +1335,20 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
         e = cudaErrorLaunchTimeout;
         break;
       }
+      // The camera rays walk warp-coherent: a warp's rays are passes of one or
+      // two pixels. (Their shadow rays gain nothing from it: a warp of them
+      // mixes lights, and lanes blocked early idle until the last ray ends,
+      // where the per-lane walk refills them.)
+      const bool coherent = packet_first && iterations == 1;
       cudaMemsetAsync(&cnt->fetch, 0, sizeof(unsigned int), stream);
       tm.start();
-      tv.extend<<<persistent_blocks(tv.extend, n, tv.block), tv.block, 0, stream>>>(scene, ps, ps.queue[cur], n, cnt);
+      if (coherent) {
+        k_extend_packet<kBlock><<<persistent_blocks(k_extend_packet<kBlock>, n), kBlock, 0, stream>>>(
+            scene, ps, ps.queue[cur], n, cnt);
+      } else {
+        tv.extend<<<persistent_blocks(tv.extend, n, tv.block), tv.block, 0, stream>>>(scene, ps, ps.queue[cur], n,
+                                                                                      cnt);
+      }
       tm.stop(st.ms_extend, st.n_extend);
       st.closest_rays += n;
       const int* shade_queue = ps.queue[cur];

@@ -124,6 +124,7 @@ class Wavefront {
  public:
   int variant = 0;  // traversal variant (see traversal_variant_info)
   bool sort_shading = true;  // shade each bounce's paths grouped by what they hit
+  bool packet_first = true;  // camera rays walk warp-coherent (traverse_packet)
   cudaError_t run(const DScene& scene, FrameParams fp, int passes, PathBuffers& buffers, cudaStream_t stream,
                   RenderStats* stats, bool timed,
                   cudaError_t (*on_chunk)(void* ctx, int first_pass, int pass_count), void* ctx);

@@ -316,6 +316,89 @@ MCRT_D void traverse_persistent(const DScene& sc, Q& q, int n, unsigned* counter
   }
 }
 
+// Warp-coherent traversal of queries [0, n): each warp takes 32 consecutive
+// queries and walks the union of their paths through the tree together, one
+// node at a time, every lane testing that node's child boxes against its own
+// ray (the node is one broadcast load). A child is entered with the lanes
+// whose ray enters its box, first the child most of those lanes reach first;
+// the other is pushed with its lane mask on a warp stack in shared memory
+// (`stack`, kStackMax entries, written by every lane with the same value).
+// Each lane thus visits exactly the nodes its own box tests admit, with the
+// same closest hit or blocking result as the per-lane walk; only the order
+// among a lane's subtrees can differ, which matters for hits at exactly equal
+// distance. With no divergence the warp runs at full width, which pays for
+// rays that share most of their paths and all run to the end: camera rays,
+// where a warp holds the passes of one or two pixels. Q is the same query
+// interface as traverse_persistent's.
+template <class Q>
+MCRT_D void traverse_packet(const DScene& sc, Q& q, int n, unsigned* counter, int2* stack, unsigned& status) {
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned bit = 1u << lane;
+  const int step_limit = max_steps(sc);
+  for (;;) {
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= static_cast<unsigned>(n)) return;
+    const bool has = base + lane < static_cast<unsigned>(n);
+    if (has) q.load(static_cast<int>(base + lane));
+    unsigned live = __ballot_sync(0xffffffffu, has);
+    int node = sc.tri_count == 0 ? kSentinel : root_ref(sc);
+    unsigned mask = live;
+    int sp = 0;
+    int steps = 0;
+    while (node != kSentinel && live != 0) {
+      mask &= live;
+      if (mask != 0) {
+        if (++steps > step_limit) {
+          if (live & bit) status |= kStatusStepLimit;
+          break;
+        }
+        if (node >= 0) {
+          const NodeRefs nd = load_node(sc.nodes, node);
+          float e0 = -1.0f, e1 = -1.0f;
+          if (mask & bit) {
+            const float tm = q.t_max();
+            const TravRay& r = q.ray();
+            e0 = box_entry(r, nd.lxy.x, nd.lxy.y, nd.lxy.z, nd.lxy.w, nd.lrz.x, nd.lrz.y, tm);
+            e1 = box_entry(r, nd.rxy.x, nd.rxy.y, nd.rxy.z, nd.rxy.w, nd.lrz.z, nd.lrz.w, tm);
+          }
+          const bool h0 = e0 >= 0.0f, h1 = e1 >= 0.0f;
+          const unsigned m0 = __ballot_sync(0xffffffffu, h0), m1 = __ballot_sync(0xffffffffu, h1);
+          if (m0 != 0 && m1 != 0) {
+            const unsigned first_left = __ballot_sync(0xffffffffu, h0 && (!h1 || e0 <= e1));
+            const bool left = 2 * __popc(first_left) >= __popc(m0 | m1);
+            if (sp < kStackMax) {
+              stack[sp] = left ? make_int2(nd.right, static_cast<int>(m1)) : make_int2(nd.left, static_cast<int>(m0));
+              sp++;
+            } else if (live & bit) {
+              status |= kStatusStackOverflow;
+            }
+            node = left ? nd.left : nd.right;
+            mask = left ? m0 : m1;
+            continue;
+          }
+          if (m0 != 0 || m1 != 0) {
+            node = m0 != 0 ? nd.left : nd.right;
+            mask = m0 | m1;
+            continue;
+          }
+        } else {
+          bool on = true;
+          if (mask & bit) on = q.leaf(~node);
+          live = __ballot_sync(0xffffffffu, (live & bit) != 0 && on);
+        }
+      }
+      if (sp == 0) break;
+      --sp;
+      const int2 e = stack[sp];
+      node = e.x;
+      mask = static_cast<unsigned>(e.y);
+    }
+    if (has) q.finish();
+  }
+}
+
 // Closest hit of one query: intersectClosest, src/bvh.ts:202-282.
 struct ClosestHit {
   int tri;
