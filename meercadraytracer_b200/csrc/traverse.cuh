@@ -40,9 +40,9 @@ constexpr int kSentinel = 0x7fffffff;  // empty stack / finished ray
 constexpr int kLeafEnd = 1 << 16;      // in tris[3k].w: last triangle of its leaf
 constexpr int kRefill = 16;            // refill a warp's finished lanes once this many are idle
 // The same threshold for the render's own kernels, measured on the mid workload
-// (closest hits: 12, shadow rays: 20, of thresholds between 4 and 32).
+// (closest hits: 12, shadow rays: 24, of thresholds between 4 and 32).
 constexpr int kRefillClosest = 12;
-constexpr int kRefillShadow = 20;
+constexpr int kRefillShadow = 24;
 
 // Status bits a kernel reports back (never a trap).
 constexpr unsigned kStatusStackOverflow = 1u;
