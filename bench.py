@@ -512,7 +512,7 @@ def run_batched(compiled: Dict[str, Any], device: int, capacity: int, seed: int 
 
 # ------------------------------------------------------------- serving loop
 def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: int, chunk: int,
-               target_ms: float = 24.0) -> Dict[str, Any]:
+               target_ms: float = 32.0) -> Dict[str, Any]:
     """The serving loop: 8 clients, two per resident scene, orbiting at 30 deg/s with Poisson
     camera moves (mean 100 ms); each move restarts the client's request: an 8x8 block preview,
     then 64 spp at 1280x720, GI on, 4 bounces. After `seconds` the moves stop and each
@@ -531,8 +531,9 @@ def run_served(compiled: Dict[str, Any], device: int, seconds: float, capacity: 
             server.add_scene(n, compiled[n])
         # The autotuner sizes chunks so one takes about `target_ms` on the slowest scene (a
         # new request's preview waits for at most the chunks in flight), unless given.
-        # 24 ms with an 8M-path pool: p99 time-to-preview near 37 ms (target 50), and the
-        # most rays per second of the settings measured (12 / 18 / 24 ms, 4M / 8M paths).
+        # 32 ms with an 8M-path pool (a chunk fills half of it): p99 time-to-preview near
+        # 40 ms (target 50). Measured 12 / 18 / 24 / 32 / 40 ms with 4M / 8M / 16M paths:
+        # rays per second grow with the chunk, and 40 ms put p99 at 47 ms.
         from meercadraytracer_b200 import autotune
         from meercadraytracer_b200.batch import RenderRequest
         from meercadraytracer_b200.compile import compile_camera
@@ -669,7 +670,7 @@ def main() -> None:
     ap.add_argument("--serve-capacity", type=int, default=1 << 23,
                     help="path pool of the serving loop (two chunks of half of it run at once)")
     ap.add_argument("--serve-chunk", type=int, default=0, help="paths per chunk in the serving loop (0: autotuned)")
-    ap.add_argument("--serve-target-ms", type=float, default=24.0,
+    ap.add_argument("--serve-target-ms", type=float, default=32.0,
                     help="serving chunk autotune: device time of one chunk on the slowest resident scene")
     ap.add_argument("--large-size", type=int, default=0, help="image side of the per-frame rebuild workload "
                                                               "(0: 2048; smaller for profiling runs)")
