@@ -88,6 +88,8 @@ BatchEngine::~BatchEngine() {
   if (lanes_.fork) cudaEventDestroy(lanes_.fork);
   destroy_graphs();
   for (int k = 0; k < kSlots; k++) {
+    if (plan_tables_dev_[k]) cudaFree(plan_tables_dev_[k]);
+    if (plan_dev_[k]) cudaFree(plan_dev_[k]);
     if (tables_dev_[k]) cudaFree(tables_dev_[k]);
     if (tables_host_[k]) cudaFreeHost(tables_host_[k]);
     if (counters_dev_[k]) cudaFree(counters_dev_[k]);
@@ -121,6 +123,7 @@ cudaError_t BatchEngine::init(int device, int capacity, size_t arena_bytes, bool
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&counters_host_[k]), sizeof(BatchCounters));
     if (e == cudaSuccess) e = cudaMemset(counters_dev_[k], 0, sizeof(BatchCounters));
     if (e == cudaSuccess) e = cudaMemset(tables_dev_[k], 0, sizeof(BatchTables));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&plan_dev_[k]), sizeof(BatchPlan));
   }
   const size_t bin_bytes = sizeof(unsigned int) * 2 * kShadeClasses * kMaxBatchScenes;
   if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&bins1_), bin_bytes);
@@ -187,6 +190,7 @@ cudaError_t BatchEngine::set_scene(int slot, const DScene& scene, int lights) {
   }
   slots_ = std::max(slots_, slots);
   graph_valid_[0] = graph_valid_[1] = false;
+  whole_valid_ = false;
   return cudaSuccess;
 }
 
@@ -198,6 +202,7 @@ cudaError_t BatchEngine::set_variant(int variant) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e == cudaSuccess) e = batch_grids(&grids_, variant, half_);
   graph_valid_[0] = graph_valid_[1] = false;
+  whole_valid_ = false;
   return e;
 }
 
@@ -209,6 +214,11 @@ void BatchEngine::destroy_graphs() {
     graph_[k] = nullptr;
     graph_valid_[k] = false;
   }
+  if (whole_exec_) cudaGraphExecDestroy(whole_exec_);
+  if (whole_graph_) cudaGraphDestroy(whole_graph_);
+  whole_exec_ = nullptr;
+  whole_graph_ = nullptr;
+  whole_valid_ = false;
 }
 
 // One graph per half of the pool and scene set: raygen, then a while node
@@ -258,6 +268,77 @@ cudaError_t BatchEngine::ensure_graph(int slot) {
   if (e == cudaSuccess) e = le;
   if (e == cudaSuccess) e = cudaGraphInstantiate(&exec_[slot], graph, 0);
   if (e == cudaSuccess) graph_valid_[slot] = true;
+  return e;
+}
+
+// One graph for whole-batch renders: per half of the pool, a while node over
+// its planned chunks whose body loads the chunk's table, generates its rays,
+// runs the bounce loop (a nested while node around the same captured
+// iteration as ensure_graph's), accumulates, and moves to the next chunk. The
+// halves' loops are independent roots, so they run side by side; each half
+// accumulates only its own requests, in chunk order.
+cudaError_t BatchEngine::ensure_whole_graph() {
+  if (whole_valid_) return cudaSuccess;
+  if (whole_exec_) cudaGraphExecDestroy(whole_exec_);
+  if (whole_graph_) cudaGraphDestroy(whole_graph_);
+  whole_exec_ = nullptr;
+  whole_graph_ = nullptr;
+  const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+  cudaError_t e = cudaGraphCreate(&whole_graph_, 0);
+  for (int k = 0; k < kSlots && e == cudaSuccess; k++) {
+    const PathState ps = slot_state(k);
+    cudaStream_t st = stream_[k];
+    cudaGraphConditionalHandle outer = 0, inner = 0;
+    e = cudaGraphConditionalHandleCreate(&outer, whole_graph_, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) break;
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = outer;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t outer_node = nullptr;
+    e = cudaGraphAddNode(&outer_node, whole_graph_, nullptr, 0, &p);
+    if (e != cudaSuccess) break;
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    // The bounce loop's condition is set by the chunk's table load.
+    e = cudaGraphConditionalHandleCreate(&inner, body, 0, 0);
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, mode);
+    if (e != cudaSuccess) break;
+    cudaError_t le = launch_batch_load_chunk(plan_dev_[k], tables_dev_[k], inner, st);
+    if (le == cudaSuccess) le = launch_batch_raygen(tables_dev_[k], ps, grids_, st);
+    e = cudaStreamEndCapture(st, &body);
+    if (e == cudaSuccess) e = le;
+    if (e != cudaSuccess) break;
+    size_t n = 0;
+    e = cudaGraphGetNodes(body, nullptr, &n);
+    std::vector<cudaGraphNode_t> head(n);
+    if (e == cudaSuccess && n > 0) e = cudaGraphGetNodes(body, head.data(), &n);
+    if (e != cudaSuccess) break;
+    cudaGraphNodeParams q{};
+    q.type = cudaGraphNodeTypeConditional;
+    q.conditional.handle = inner;
+    q.conditional.type = cudaGraphCondTypeWhile;
+    q.conditional.size = 1;
+    cudaGraphNode_t inner_node = nullptr;
+    e = cudaGraphAddNode(&inner_node, body, head.data(), n, &q);
+    if (e != cudaSuccess) break;
+    cudaGraph_t loop = q.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(st, loop, nullptr, nullptr, 0, mode);
+    if (e != cudaSuccess) break;
+    le = launch_batch_iteration(scenes_, nscenes_, tables_dev_[k], ps, paths_.capacity(), paths_.slots(),
+                                counters_dev_[k], grids_, true, inner, st, &lanes_);
+    e = cudaStreamEndCapture(st, &loop);
+    if (e == cudaSuccess) e = le;
+    if (e != cudaSuccess) break;
+    e = cudaStreamBeginCaptureToGraph(st, body, &inner_node, nullptr, 1, mode);
+    if (e != cudaSuccess) break;
+    le = launch_batch_accumulate(tables_dev_[k], ps, grids_, st);
+    if (le == cudaSuccess) le = launch_batch_next_chunk(plan_dev_[k], outer, st);
+    e = cudaStreamEndCapture(st, &body);
+    if (e == cudaSuccess) e = le;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&whole_exec_, whole_graph_, 0);
+  if (e == cudaSuccess) whole_valid_ = true;
   return e;
 }
 
@@ -337,6 +418,7 @@ void BatchEngine::plan(Chunk& c) {
   for (auto& rp : requests_) {
     Request& r = *rp;
     if (!active(r) || r.preview != 1 || static_cast<int>(c.segs.size()) >= kMaxSegments) continue;
+    if (plan_branch_ >= 0 && r.branch != plan_branch_) continue;
     const int b = r.d.preview_block;
     const long long blocks = static_cast<long long>((r.d.fp.width + b - 1) / b) * ((r.d.fp.height + b - 1) / b);
     // A preview larger than the chunk size (never than half the pool:
@@ -348,6 +430,7 @@ void BatchEngine::plan(Chunk& c) {
   for (auto& rp : requests_) {
     Request& r = *rp;
     if (!active(r) || r.preview == 1 || static_cast<int>(c.segs.size()) >= kMaxSegments) continue;
+    if (plan_branch_ >= 0 && r.branch != plan_branch_) continue;
     if (std::find(used.begin(), used.end(), &r) != used.end()) continue;
     if (r.next_pass >= r.d.samples || room <= 0) continue;
     const long long P = r.pixels();
@@ -383,10 +466,7 @@ void BatchEngine::plan(Chunk& c) {
   for (SegmentPlan& s : c.segs) s.r->inflight++;
 }
 
-cudaError_t BatchEngine::launch(Chunk& c) {
-  const int k = c.slot;
-  cudaStream_t st = stream_[k];
-  BatchTables* T = tables_host_[k];
+void BatchEngine::fill_tables(const Chunk& c, BatchTables* T) {
   const int nseg = static_cast<int>(c.segs.size());
   T->segments = nseg;
   T->iteration = 0;
@@ -434,7 +514,14 @@ cudaError_t BatchEngine::launch(Chunk& c) {
   T->paths = paths;
   // Paths end by bounce count or after kMaxPassThrough pass-throughs per bounce.
   T->max_iterations = (max_bounces + 1) * (kMaxPassThrough + 1) + 2;
-  const size_t bytes = offsetof(BatchTables, fp) + sizeof(FrameParams) * static_cast<size_t>(nseg);
+}
+
+cudaError_t BatchEngine::launch(Chunk& c) {
+  const int k = c.slot;
+  cudaStream_t st = stream_[k];
+  BatchTables* T = tables_host_[k];
+  fill_tables(c, T);
+  const size_t bytes = offsetof(BatchTables, fp) + sizeof(FrameParams) * static_cast<size_t>(T->segments);
 
   cudaError_t e = cudaSuccess;
   if (!c.start) e = cudaEventCreate(&c.start);
@@ -578,6 +665,136 @@ cudaError_t BatchEngine::step(std::vector<BatchEvent>& events, bool* idle, bool*
   for (const auto& r : requests_)
     if (!r->cancelled && !r->finished) pending = true;
   if (idle) *idle = !pending && inflight_.empty();
+  return cudaSuccess;
+}
+
+// The most chunks a whole-batch render plans per half before it calls the
+// plan a scheduling fault.
+constexpr size_t kMaxPlannedChunks = 1 << 16;
+
+cudaError_t BatchEngine::render_whole(std::vector<BatchEvent>& events, bool* rendered) {
+  *rendered = false;
+  cudaError_t e = cudaSetDevice(device_);
+  if (e != cudaSuccess) return e;
+  if (!use_graph_ || !inflight_.empty()) return cudaSuccess;
+  std::vector<Request*> todo;
+  for (auto& rp : requests_) {
+    Request& r = *rp;
+    if (r.cancelled || r.finished) continue;
+    const bool started = r.next_pass > 0 || r.next_pix > 0 || r.preview == 2 || r.inflight > 0;
+    if (started || r.host_progress || (r.host_preview && r.d.preview_block > 1)) return cudaSuccess;
+    todo.push_back(&r);
+  }
+  if (todo.empty()) return cudaSuccess;
+  for (Request* r : todo)
+    if (!r->admitted && !admit(*r)) return cudaSuccess;  // step() admits the rest as room frees up
+
+  // The halves take the requests by samples (pixels x passes), largest first,
+  // each to the half with fewer so far.
+  std::vector<Request*> order = todo;
+  auto work = [](const Request* r) { return r->pixels() * std::max(1, r->d.samples); };
+  std::stable_sort(order.begin(), order.end(), [&](const Request* a, const Request* b) { return work(a) > work(b); });
+  long long load[kSlots] = {};
+  for (Request* r : order) {
+    const int b = load[0] <= load[1] ? 0 : 1;
+    r->branch = b;
+    load[b] += work(r);
+  }
+  std::vector<Chunk> chunks[kSlots];
+  for (int b = 0; b < kSlots; b++) {
+    plan_branch_ = b;
+    for (;;) {
+      Chunk c;
+      c.slot = b;
+      plan(c);
+      if (c.segs.empty()) break;
+      chunks[b].push_back(std::move(c));
+      if (chunks[b].size() > kMaxPlannedChunks) break;
+    }
+  }
+  plan_branch_ = -1;
+  // After planning, a failure drops these requests (their passes are taken):
+  // the caller gets the error and their buffers return to the arena.
+  auto abandon = [&](cudaError_t err) {
+    for (Request* r : todo) {
+      r->cancelled = true;
+      r->inflight = 0;
+      r->branch = -1;
+    }
+    for (auto it = requests_.begin(); it != requests_.end();) {
+      if ((*it)->cancelled) {
+        release(**it);
+        it = requests_.erase(it);
+      } else {
+        ++it;
+      }
+    }
+    return err;
+  };
+  for (Request* r : todo)
+    if (r->next_pass < r->d.samples || r->preview == 1) return abandon(cudaErrorInvalidValue);  // a stalled plan
+
+  // Every table of each half in one upload, then one graph launch.
+  for (int b = 0; b < kSlots && e == cudaSuccess; b++) {
+    const size_t n = std::max<size_t>(1, chunks[b].size());
+    if (plan_tables_cap_[b] < n) {
+      if (plan_tables_dev_[b]) cudaFree(plan_tables_dev_[b]);
+      plan_tables_dev_[b] = nullptr;
+      plan_tables_cap_[b] = 0;
+      e = cudaMalloc(reinterpret_cast<void**>(&plan_tables_dev_[b]), n * sizeof(BatchTables));
+      if (e != cudaSuccess) break;
+      plan_tables_cap_[b] = n;
+    }
+    std::vector<BatchTables> host(n);  // zeroed: an empty table when the half has no chunk
+    for (size_t i = 0; i < chunks[b].size(); i++) fill_tables(chunks[b][i], &host[i]);
+    e = cudaMemcpy(plan_tables_dev_[b], host.data(), n * sizeof(BatchTables), cudaMemcpyHostToDevice);
+    const BatchPlan pl{plan_tables_dev_[b], static_cast<int>(n), 0};
+    if (e == cudaSuccess) e = cudaMemcpy(plan_dev_[b], &pl, sizeof(BatchPlan), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = ensure_whole_graph();
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&ev1);
+  cudaStream_t st = stream_[0];
+  if (e == cudaSuccess) e = cudaEventRecord(ev0, st);
+  if (e == cudaSuccess) e = cudaGraphLaunch(whole_exec_, st);
+  if (e == cudaSuccess) e = cudaEventRecord(ev1, st);
+  for (Request* r : todo)
+    if (e == cudaSuccess && r->host_image)
+      e = cudaMemcpyAsync(r->host_image, r->image, static_cast<size_t>(r->pixels()) * 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  float ms = 0;
+  if (e == cudaSuccess && cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) totals_.gpu_ms += ms;
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (e != cudaSuccess) return abandon(e);
+  totals_.graph_launches++;
+  totals_.chunks += chunks[0].size() + chunks[1].size();
+  for (int k = 0; k < kSlots; k++) {
+    e = cudaMemcpy(counters_host_[k], counters_dev_[k], sizeof(BatchCounters), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return e;
+    slot_totals_[k] = *counters_host_[k];
+    totals_.status |= slot_totals_[k].status;
+  }
+  totals_.closest = slot_totals_[0].closest + slot_totals_[1].closest;
+  totals_.any = slot_totals_[0].any + slot_totals_[1].any;
+  for (Request* r : todo) {
+    if (r->preview == 2) events.push_back(BatchEvent{r->id, kEventPreview, 0});
+    events.push_back(BatchEvent{r->id, kEventDone, r->d.samples});
+    r->finished = true;
+    r->inflight = 0;
+    r->branch = -1;
+  }
+  for (auto it = requests_.begin(); it != requests_.end();) {
+    Request& r = **it;
+    if ((r.finished || r.cancelled) && r.inflight == 0) {
+      release(r);
+      it = requests_.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  *rendered = true;
   return cudaSuccess;
 }
 

@@ -94,6 +94,17 @@ class BatchEngine {
   // or finished; a step that does neither while not idle is a scheduling
   // fault, which callers report instead of stepping again.
   cudaError_t step(std::vector<BatchEvent>& events, bool* idle, bool* progressed = nullptr);
+  // Renders every queued request to completion as one graph launch: the
+  // requests are split between the two halves of the pool, each half's
+  // chunks are planned ahead and uploaded at once, and each half runs its
+  // chunks in order in a device-driven loop (raygen, the bounce loop,
+  // accumulation), the two halves side by side. Appends a done event (and a
+  // preview event for a request with a block preview) per request.
+  // *rendered is false, and nothing is launched, when a chunk is in flight,
+  // graphs are off, a request wants its block preview or progress images
+  // delivered while it runs, or the arena cannot hold every request at once;
+  // step() then renders them.
+  cudaError_t render_whole(std::vector<BatchEvent>& events, bool* rendered);
   BatchTotals totals() const { return totals_; }
   int capacity() const { return capacity_; }
   // The most paths one chunk holds: half the pool (two chunks run at once).
@@ -129,6 +140,7 @@ class BatchEngine {
     int next_pass = 0;        // first pass not yet scheduled
     int next_pix = 0;         // first pixel of the pass group at next_pass not yet scheduled
     int group = 0;            // passes of that group while it is split by pixel range
+    int branch = -1;          // half of the pool a whole-batch render gives it (render_whole)
     int inflight = 0;         // chunks in flight that hold a segment of this request
     int copying = 0;          // chunks in flight copying this request's image to the host
     long long pixels() const { return static_cast<long long>(d.fp.width) * d.fp.height; }
@@ -150,9 +162,12 @@ class BatchEngine {
 
   PathState slot_state(int slot) const;
   cudaError_t ensure_graph(int slot);
+  cudaError_t ensure_whole_graph();
   void destroy_graphs();
   bool admit(Request& r);
   void plan(Chunk& c);
+  // The chunk's tables as its kernels read them (host copy).
+  void fill_tables(const Chunk& c, BatchTables* T);
   cudaError_t launch(Chunk& c);
   cudaError_t finish(Chunk& c, std::vector<BatchEvent>& events);
   void release(Request& r);
@@ -180,6 +195,15 @@ class BatchEngine {
   cudaGraph_t graph_[kSlots] = {};
   cudaGraphExec_t exec_[kSlots] = {};
   bool graph_valid_[kSlots] = {};
+  // Whole-batch renders: per half, the planned chunks' tables and the loop
+  // state, and one graph running both halves' chunk loops.
+  int plan_branch_ = -1;  // plan() takes only this half's requests (>= 0)
+  BatchTables* plan_tables_dev_[kSlots] = {};
+  size_t plan_tables_cap_[kSlots] = {};  // tables the allocation holds
+  BatchPlan* plan_dev_[kSlots] = {};
+  cudaGraph_t whole_graph_ = nullptr;
+  cudaGraphExec_t whole_exec_ = nullptr;
+  bool whole_valid_ = false;
   long long next_id_ = 1;
   std::deque<std::unique_ptr<Request>> requests_;  // submission order
   std::deque<Chunk> inflight_;

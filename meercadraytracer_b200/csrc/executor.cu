@@ -1425,6 +1425,19 @@ int32_t mcrt_batch_render(mcrt_batch* b, int32_t count, const mcrt_request* requ
     checked_batch(b);
     if (count < 0 || (count > 0 && !requests)) fail(MCRT_ERR_INVALID, "bad request list");
     for (int i = 0; i < count; i++) submit_request(b, requests + i);
+    // The whole batch as one graph launch when no request needs host work
+    // between chunks (BatchEngine::render_whole); otherwise, or for what is
+    // left, chunk by chunk.
+    {
+      check_slots(b);
+      std::vector<BatchEvent> ev;
+      const unsigned earlier = b->engine.totals().status;
+      bool rendered = false;
+      cuda_check(b->engine.render_whole(ev, &rendered), "whole-batch render");
+      if (b->engine.totals().status & kStatusIterationLimit)
+        fail(MCRT_ERR_CUDA, "a batched chunk did not finish within its iteration limit");
+      check_walk(b->engine.totals().status & ~earlier);
+    }
     // Every step launches or finishes a chunk until the engine is idle, so
     // this loop ends; a step that does neither is a scheduling fault and fails
     // the call rather than spinning.

@@ -20,6 +20,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -1777,6 +1778,39 @@ cudaError_t launch_batch_iteration(const DScene* scenes, int nscenes, BatchTable
 
 cudaError_t launch_batch_accumulate(const BatchTables* t, const PathState& ps, const BatchGrids& g, cudaStream_t s) {
   k_batch_accumulate<<<g.accumulate, 256, 0, s>>>(t, ps);
+  return cudaGetLastError();
+}
+
+// The used part of the plan's current table (its fixed fields and the
+// segments' frame parameters), copied word by word into the chunk's table.
+__global__ void k_batch_load_chunk(const BatchPlan* plan, BatchTables* dst, cudaGraphConditionalHandle inner) {
+  const int c = min(plan->index, plan->count - 1);
+  const BatchTables* src = plan->tables + c;
+  const size_t bytes = offsetof(BatchTables, fp) + sizeof(FrameParams) * static_cast<size_t>(src->segments);
+  const int words = static_cast<int>(bytes / sizeof(int));
+  const int* from = reinterpret_cast<const int*>(src);
+  int* to = reinterpret_cast<int*>(dst);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x) to[i] = from[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(inner, 1u);
+}
+
+__global__ void k_batch_next_chunk(BatchPlan* plan, cudaGraphConditionalHandle outer) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const int next = plan->index + 1;
+  plan->index = next;
+  cudaGraphSetConditional(outer, next < plan->count ? 1u : 0u);
+}
+
+cudaError_t launch_batch_load_chunk(const BatchPlan* plan, BatchTables* dst, cudaGraphConditionalHandle inner,
+                                    cudaStream_t s) {
+  static_assert(offsetof(BatchTables, fp) % sizeof(int) == 0 && sizeof(FrameParams) % sizeof(int) == 0,
+                "tables are copied in 4-byte words");
+  k_batch_load_chunk<<<8, 256, 0, s>>>(plan, dst, inner);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_next_chunk(BatchPlan* plan, cudaGraphConditionalHandle outer, cudaStream_t s) {
+  k_batch_next_chunk<<<1, 32, 0, s>>>(plan, outer);
   return cudaGetLastError();
 }
 

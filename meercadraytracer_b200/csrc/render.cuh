@@ -228,6 +228,21 @@ cudaError_t launch_batch_iteration(const DScene* scenes, int nscenes, BatchTable
 // the requests' images.
 cudaError_t launch_batch_accumulate(const BatchTables* t, const PathState& ps, const BatchGrids& g, cudaStream_t s);
 
+// A whole batch planned ahead for one half of the pool: its chunks' tables in
+// order (sizeof(BatchTables) apart, at least one, an empty table when the half
+// has no work) and the chunk that runs now.
+struct BatchPlan {
+  const BatchTables* tables;
+  int count;
+  int index;
+};
+// Copies the current chunk's table into `dst`, where the chunk's kernels read
+// it, and opens the bounce loop (`inner` = 1).
+cudaError_t launch_batch_load_chunk(const BatchPlan* plan, BatchTables* dst, cudaGraphConditionalHandle inner,
+                                    cudaStream_t s);
+// Moves to the next chunk; `outer` = 1 while chunks remain.
+cudaError_t launch_batch_next_chunk(BatchPlan* plan, cudaGraphConditionalHandle outer, cudaStream_t s);
+
 // Kernel launchers used by the executor.
 cudaError_t launch_accumulate(const float4* samples, int npix, int passes_in_chunk, float4* sum, int total_passes,
                               int last_chunk, uint8_t* image, const FrameParams& fp, int srgb, cudaStream_t s);

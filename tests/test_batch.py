@@ -78,6 +78,27 @@ def test_batch_matches_plain_renders(two_scenes, capacity):
         renderer.dispose()
 
 
+def test_whole_batch_is_one_graph_launch(two_scenes):
+    # mcrt_batch_render plans every chunk ahead and runs them all as one graph
+    # launch, the two halves of the pool side by side; the images are still the
+    # plain renders', and a second batch reuses the graph (one more launch).
+    renderer = BatchRenderer(capacity=6000, memory_budget=64 << 20)
+    try:
+        reqs = _requests(two_scenes)
+        images = renderer.render(reqs)
+        st = renderer.stats()
+        assert st["graph_launches"] == 1 and st["chunks"] > 2 and st["status"] == 0
+        assert st["arena_used"] == 0
+        for r, img in zip(reqs, images):
+            assert np.array_equal(img, _plain(renderer, r))
+        again = renderer.render(reqs[1:4])
+        assert renderer.stats()["graph_launches"] == 2
+        for r, img in zip(reqs[1:4], again):
+            assert np.array_equal(img, _plain(renderer, r))
+    finally:
+        renderer.dispose()
+
+
 def test_request_alone_equals_request_in_mix(two_scenes):
     reqs = _requests(two_scenes)
     alone = BatchRenderer(capacity=1 << 15, memory_budget=64 << 20)
