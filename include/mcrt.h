@@ -337,7 +337,13 @@ int32_t mcrt_batch_cancel(mcrt_batch* batch, int64_t id);
  * max_events events; *idle is 1 when nothing is queued or in flight. */
 int32_t mcrt_batch_step(mcrt_batch* batch, mcrt_batch_event* events, int32_t max_events, int32_t* n_events,
                         int32_t* idle);
-/* Submits `count` requests and runs until all are done. */
+/* Submits `count` requests and runs until all are done. When nothing else is
+ * queued, every request fits the arena at once and none asks for a
+ * preview_image or progress_image, the whole batch runs as one CUDA graph
+ * launch (every chunk planned ahead, the requests split between the two
+ * halves of the pool, each half's chunks run in a device-driven loop);
+ * otherwise chunk by chunk as mcrt_batch_step runs them. Images are the
+ * same either way. */
 int32_t mcrt_batch_render(mcrt_batch* batch, int32_t count, const mcrt_request* requests);
 int32_t mcrt_batch_get_stats(mcrt_batch* batch, mcrt_batch_stats* out);
 
