@@ -147,16 +147,29 @@ __global__ void __launch_bounds__(kBlock) k_raygen(FrameParams fp, PathState ps,
   if (pid < n) raygen_path(fp, ps, pid);
 }
 
+// Shading class of a hit on material m (the shading-order sort's key): 1 +
+// 2 x the material model + 1 if transmissive; a miss is class 0.
+MCRT_D int material_class(const DScene& sc, int m) {
+  const DMaterial& mat = sc.materials[m];
+  return 1 + 2 * min(max(mat.model, 0), 6) + (mat.transmission > 0.0f ? 1 : 0);
+}
+
 // ------------------------------------------------------------------ extend
 // Closest hit of each queued path's ray (intersectClosest, bvh.ts:202-282),
 // persistent: warps take rays from cnt->fetch until the queue is drained.
+// With `hist` (shared memory, kShadeClasses counters) each finished query
+// also stores its hit's shading class by queue position (ps.cls) and counts
+// it, the first half of the shading-order sort.
 struct ExtendQuery {
   const DScene& sc;
   const PathState& ps;
   const int* queue;
   int pid;
   ClosestState cs;
+  unsigned int* hist;
+  int qi;
   MCRT_D void load(int i) {
+    qi = i;
     pid = queue[i];
     const float4 o = ps.ray_o[pid], d = ps.ray_d[pid];
     cs.start(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, (ps.flags[pid] & kFlagCull) != 0);
@@ -168,6 +181,29 @@ struct ExtendQuery {
     const ClosestHit& h = cs.h;
     const unsigned word = h.tri >= 0 ? ((h.front ? 0x80000000u : 0u) | static_cast<unsigned>(h.tri + 1)) : 0u;
     ps.hit[pid] = make_float4(h.t, h.u, h.v, __uint_as_float(word));
+    if (hist) {
+      const int c = h.tri >= 0 ? material_class(sc, h.material) : 0;
+      ps.cls[qi] = static_cast<uint8_t>(c);
+      atomicAdd(hist + c, 1u);
+    }
+  }
+};
+
+// The shared histogram of a closest-hit kernel that counts shading classes
+// (`bins` given): cleared before the walk, added to `bins` after it.
+struct ClassHistogram {
+  unsigned int* bins;
+  unsigned int* hist;
+  MCRT_D unsigned int* begin() {
+    if (!bins) return nullptr;
+    if (threadIdx.x < kShadeClasses) hist[threadIdx.x] = 0;
+    __syncthreads();
+    return hist;
+  }
+  MCRT_D void end() {
+    if (!bins) return;
+    __syncthreads();
+    if (threadIdx.x < kShadeClasses && hist[threadIdx.x]) atomicAdd(bins + threadIdx.x, hist[threadIdx.x]);
   }
 };
 
@@ -176,23 +212,29 @@ struct ExtendQuery {
 // and buys a ninth more resident warps than the unconstrained 56 registers.
 template <int B, int S>
 __global__ void __launch_bounds__(B, 1280 / B) k_extend(DScene sc, PathState ps, const int* __restrict__ queue, int n,
-                                              Counters* cnt) {
+                                              Counters* cnt, unsigned int* bins) {
+  __shared__ unsigned int hist[kShadeClasses];
+  ClassHistogram ch{bins, hist};
   unsigned status = 0;
-  ExtendQuery q{sc, ps, queue, 0, {}};
+  ExtendQuery q{sc, ps, queue, 0, {}, ch.begin(), 0};
   walk<kRefillClosest, B, S>(sc, q, n, &cnt->fetch, status);
   if (status) atomicOr(&cnt->status, status);
+  ch.end();
 }
 
 // The same over a queue of coherent rays (the camera rays), warp by warp
 // (traverse_packet); B / 32 warp stacks of kStackMax entries in shared memory.
 template <int B>
 __global__ void __launch_bounds__(B) k_extend_packet(DScene sc, PathState ps, const int* __restrict__ queue, int n,
-                                                     Counters* cnt) {
+                                                     Counters* cnt, unsigned int* bins) {
   __shared__ int2 stack[(B / 32) * kStackMax];
+  __shared__ unsigned int hist[kShadeClasses];
+  ClassHistogram ch{bins, hist};
   unsigned status = 0;
-  ExtendQuery q{sc, ps, queue, 0, {}};
+  ExtendQuery q{sc, ps, queue, 0, {}, ch.begin(), 0};
   traverse_packet(sc, q, n, &cnt->fetch, stack + (threadIdx.x >> 5) * kStackMax, status);
   if (status) atomicOr(&cnt->status, status);
+  ch.end();
 }
 
 // ------------------------------------------------------- shading order
@@ -205,24 +247,7 @@ MCRT_D int shade_class(const DScene& sc, const PathState& ps, int pid) {
   const unsigned word = __float_as_uint(__ldg(reinterpret_cast<const float*>(ps.hit + pid) + 3));
   const int tri = static_cast<int>(word & 0x7fffffffu) - 1;
   if (tri < 0) return 0;
-  const int m = __float_as_int(__ldg(&sc.tris[3 * static_cast<size_t>(tri) + 1].w));
-  const DMaterial& mat = sc.materials[m];
-  return 1 + 2 * min(max(mat.model, 0), 6) + (mat.transmission > 0.0f ? 1 : 0);
-}
-
-__global__ void __launch_bounds__(256) k_class_count(DScene sc, PathState ps, const int* __restrict__ queue, int n,
-                                                     unsigned int* __restrict__ bins) {
-  __shared__ unsigned int h[kShadeClasses];
-  if (threadIdx.x < kShadeClasses) h[threadIdx.x] = 0;
-  __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) {
-    const int c = shade_class(sc, ps, queue[i]);
-    ps.cls[i] = static_cast<uint8_t>(c);  // kept for the scatter, by queue position
-    atomicAdd(&h[c], 1u);
-  }
-  __syncthreads();
-  if (threadIdx.x < kShadeClasses && h[threadIdx.x]) atomicAdd(&bins[threadIdx.x], h[threadIdx.x]);
+  return material_class(sc, __float_as_int(__ldg(&sc.tris[3 * static_cast<size_t>(tri) + 1].w)));
 }
 
 // Places the block's tile [first, first + blockDim.x) of the queue: ranks
@@ -1242,7 +1267,7 @@ int persistent_blocks(K kernel, long long n, int block = kBlock) {
 
 // The traversal kernels compiled for each variant (block size, short-stack
 // depth); the autotuner picks one per scene and workload.
-using ExtendFn = void (*)(DScene, PathState, const int*, int, Counters*);
+using ExtendFn = void (*)(DScene, PathState, const int*, int, Counters*, unsigned int*);
 using ShadowFn = void (*)(DScene, PathState, int, int, Counters*);
 
 struct PlainVariant {
@@ -1345,24 +1370,28 @@ cudaError_t Wavefront::run(const DScene& scene, FrameParams fp, int passes, Path
       // walk refills them.)
       const int warp_pixels = 32 / std::max(1, std::min(f.npass, 32));
       const bool coherent = packet_first && iterations == 1 && warp_pixels * 360 <= f.height;
+      // A queue long enough to shade in hit-class order has its classes
+      // counted by the closest-hit kernel itself (ExtendQuery with a
+      // histogram); the scatter then puts the queue in that order.
+      const bool sort = sort_shading && n >= kSortMin;
+      unsigned int* class_bins = sort ? ps.bins : nullptr;
+      if (sort) cudaMemsetAsync(ps.bins, 0, 2 * kShadeClasses * sizeof(unsigned int), stream);
       cudaMemsetAsync(&cnt->fetch, 0, sizeof(unsigned int), stream);
       tm.start();
       if (coherent) {
         k_extend_packet<kBlock><<<persistent_blocks(k_extend_packet<kBlock>, n), kBlock, 0, stream>>>(
-            scene, ps, ps.queue[cur], n, cnt);
+            scene, ps, ps.queue[cur], n, cnt, class_bins);
       } else {
         tv.extend<<<persistent_blocks(tv.extend, n, tv.block), tv.block, 0, stream>>>(scene, ps, ps.queue[cur], n,
-                                                                                      cnt);
+                                                                                      cnt, class_bins);
       }
       tm.stop(st.ms_extend, st.n_extend);
       st.closest_rays += n;
       const int* shade_queue = ps.queue[cur];
-      if (sort_shading && n >= kSortMin) {
-        cudaMemsetAsync(ps.bins, 0, 2 * kShadeClasses * sizeof(unsigned int), stream);
-        k_class_count<<<blocks_for(n, 256), 256, 0, stream>>>(scene, ps, ps.queue[cur], n, ps.bins);
+      if (sort) {
         k_class_scatter<<<blocks_for(n, 256), 256, 0, stream>>>(scene, ps, ps.queue[cur], n, ps.bins, ps.binned);
         shade_queue = ps.binned;
-        st.launches += 2;
+        st.launches += 1;
       }
       join_side();
       cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), stream);
@@ -1434,7 +1463,7 @@ cudaError_t primary_hits(const DScene& scene, FrameParams fp, PathBuffers& buffe
   cudaMemsetAsync(&buffers.counters()->fetch, 0, sizeof(unsigned int), stream);
   const PlainVariant& tv = plain_variant(0);
   tv.extend<<<persistent_blocks(tv.extend, n, tv.block), tv.block, 0, stream>>>(scene, ps, ps.queue[0], n,
-                                                                                  buffers.counters());
+                                                                                  buffers.counters(), nullptr);
   return cudaGetLastError();
 }
 
@@ -1504,7 +1533,7 @@ __global__ void __launch_bounds__(B, 1280 / B) k_batch_extend(DScene sc, int s, 
   const int n = static_cast<int>(sq->count);
   if (n == 0) return;
   unsigned status = 0;
-  ExtendQuery q{sc, ps, ps.queue[t->iteration & 1] + sq->base, 0, {}};
+  ExtendQuery q{sc, ps, ps.queue[t->iteration & 1] + sq->base, 0, {}, nullptr, 0};
   walk<kRefillClosest, B, S>(sc, q, n, &sq->fetch, status);
   if (status) atomicOr(&bc->status, status);
 }
@@ -1568,8 +1597,9 @@ __global__ void __launch_bounds__(kBlock) k_batch_resolve(DScene sc, int s, Batc
   }
 }
 
-// Shading order of one scene's queue range (k_class_count / k_class_scatter
-// over a resident grid): bins of scene s are bins[32 s, 32 s + 32).
+// Shading order of one scene's queue range (the class count, then
+// k_class_scatter's scatter, over a resident grid): bins of scene s are
+// bins[32 s, 32 s + 32).
 __global__ void __launch_bounds__(256) k_batch_class_count(DScene sc, int s, BatchTables* t, PathState ps) {
   SceneQueues* sq = &t->scenes[s];
   const int n = static_cast<int>(sq->count);

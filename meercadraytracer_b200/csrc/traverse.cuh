@@ -404,6 +404,7 @@ struct ClosestHit {
   int tri;
   float t, u, v;
   bool front;
+  int material;  // the hit triangle's material (its tris[3k + 1].w)
 };
 
 struct ClosestState {
@@ -416,7 +417,7 @@ struct ClosestState {
     tmax = __int_as_float(0x7f800000);
     cull = c;
     tests = 0;
-    h = ClosestHit{-1, 0.0f, 0.0f, 0.0f, true};
+    h = ClosestHit{-1, 0.0f, 0.0f, 0.0f, true, 0};
   }
   int tests;
   MCRT_D bool leaf(const DScene& sc, int first) {
@@ -428,7 +429,7 @@ struct ClosestState {
       TriHit th;
       if (intersect_triangle(r, a, b, c, tmax, cull ? tri_side(w0.w) : 2, th)) {
         tmax = th.t;
-        h = ClosestHit{k, th.t, th.u, th.v, th.front};
+        h = ClosestHit{k, th.t, th.u, th.v, th.front, __float_as_int(w1.w)};
       }
       if (leaf_end(w0.w)) break;
     }
