@@ -673,7 +673,7 @@ def main() -> None:
     ap.add_argument("--large-only", action="store_true",
                     help="run only the per-frame rebuild workload and print its record (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop run")
-    ap.add_argument("--batch-capacity", type=int, default=1 << 25,
+    ap.add_argument("--batch-capacity", type=int, default=1 << 26,
                     help="path pool of the batch engine (two chunks of half of it run at once)")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the served client simulation")
     ap.add_argument("--serve-capacity", type=int, default=1 << 23,
