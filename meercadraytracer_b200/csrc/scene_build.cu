@@ -13,12 +13,13 @@
 // partitions here are stable.
 #include <cuda_runtime.h>
 
+#include <cub/block/block_reduce.cuh>
 #include <cub/block/block_scan.cuh>
-#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1181,6 +1182,89 @@ __global__ void k_reorder_f32(const uint32_t* __restrict__ order, int n, const f
   sides_out[i] = sides[s];
 }
 
+// Exclusive prefix sums of up to kScanMax int arrays of the same length n, in
+// two launches over a fixed grid of kScanBlocks blocks, each owning one
+// contiguous segment of every array: k_scan_sums adds up each block's
+// segments; k_scan_write gives each block the sums of the blocks before it
+// and scans its segments tile by tile. Integer sums are exact in any order,
+// so the results are those of a sequential scan.
+constexpr int kScanMax = 4;
+constexpr int kScanBlocks = 4 * 148;
+constexpr int kScanThreads = 256;
+
+struct ScanArrays {
+  const int* in[kScanMax];
+  int* out[kScanMax];
+  int count;
+};
+
+__device__ __forceinline__ void scan_segment(int n, int& lo, int& hi) {
+  const int seg = (n + kScanBlocks - 1) / kScanBlocks;
+  lo = min(n, static_cast<int>(blockIdx.x) * seg);
+  hi = min(n, lo + seg);
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(ScanArrays a, int n, int* __restrict__ sums) {
+  using Reduce = cub::BlockReduce<int, kScanThreads>;
+  __shared__ typename Reduce::TempStorage tmp;
+  int lo, hi;
+  scan_segment(n, lo, hi);
+  for (int k = 0; k < a.count; k++) {
+    int v = 0;
+    for (int i = lo + static_cast<int>(threadIdx.x); i < hi; i += kScanThreads) v += a.in[k][i];
+    const int total = Reduce(tmp).Sum(v);
+    if (threadIdx.x == 0) sums[k * kScanBlocks + blockIdx.x] = total;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_write(ScanArrays a, int n, const int* __restrict__ sums) {
+  using Reduce = cub::BlockReduce<int, kScanThreads>;
+  using Scan = cub::BlockScan<int, kScanThreads>;
+  __shared__ union {
+    typename Reduce::TempStorage reduce;
+    typename Scan::TempStorage scan;
+  } tmp;
+  __shared__ int base;
+  int lo, hi;
+  scan_segment(n, lo, hi);
+  for (int k = 0; k < a.count; k++) {
+    int before = 0;
+    for (int b = static_cast<int>(threadIdx.x); b < static_cast<int>(blockIdx.x); b += kScanThreads)
+      before += sums[k * kScanBlocks + b];
+    const int offset = Reduce(tmp.reduce).Sum(before);
+    if (threadIdx.x == 0) base = offset;
+    __syncthreads();
+    int running = base;
+    for (int tile = lo; tile < hi; tile += kScanThreads) {
+      const int i = tile + static_cast<int>(threadIdx.x);
+      const int v = i < hi ? a.in[k][i] : 0;
+      int ex = 0, total = 0;
+      Scan(tmp.scan).ExclusiveSum(v, ex, total);
+      if (i < hi) a.out[k][i] = running + ex;
+      running += total;
+      __syncthreads();
+    }
+    __syncthreads();  // every thread has read `base` before the next array rewrites it
+  }
+}
+
+// Exclusive sums of in[k] into out[k] (k < count <= kScanMax), each of length
+// n; `sums` holds kScanMax * kScanBlocks ints.
+void scan_arrays(std::initializer_list<const int*> in, std::initializer_list<int*> out, int n, int* sums,
+                 cudaStream_t s) {
+  ScanArrays a{};
+  a.count = static_cast<int>(in.size());
+  if (a.count > kScanMax || out.size() != in.size()) throw std::runtime_error("scan_arrays: bad array count");
+  int k = 0;
+  for (const int* p : in) a.in[k++] = p;
+  k = 0;
+  for (int* p : out) a.out[k++] = p;
+  if (n <= 0) return;
+  k_scan_sums<<<kScanBlocks, kScanThreads, 0, s>>>(a, n, sums);
+  k_scan_write<<<kScanBlocks, kScanThreads, 0, s>>>(a, n, sums);
+}
+
 }  // namespace
 
 struct BuildBuffers {
@@ -1191,7 +1275,7 @@ struct BuildBuffers {
   DevArray<int> is_split, rank;
   DevArray<int> nb, boff, wide, wid, blk_left, blk_pre, totals, live, live_pos, small, spos, tiny, tpos, slist;
   DevArray<WideAcc> acc;
-  DevArray<uint8_t> scan_tmp;
+  DevArray<int> scan_sums;  // per-block sums of the level plan's prefix sums (scan_arrays)
   DevArray<int> host_pair;
   // compile
   DevArray<double> p, nrm, uv, colors, box;
@@ -1247,19 +1331,14 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
   k_prepare<<<blocks_of(n, 256), 256, 0, s>>>(d_tris, n, bmin, bmax, cent, d_order);
   Slot root{0, 0, n, 0};
   check(cudaMemcpyAsync(slots[0], &root, sizeof(Slot), cudaMemcpyHostToDevice, s), "upload");
-  size_t scan_bytes = 0;
-  check(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, blk_left, blk_pre, max_blocks, s), "scan");
-  uint8_t* scan_tmp = B.scan_tmp.ensure(scan_bytes);
+  int* scan_sums = B.scan_sums.ensure(kScanMax * kScanBlocks);
   int active = 1, total = 1, cur = 0;
   uint32_t* order_a = d_order;
   uint32_t* order_b = tmp;
   int pair[2], tot[4], lives[2];
   while (active > 0) {
     k_level_plan<<<blocks_of(active, 256), 256, 0, s>>>(slots[cur], active, nbk, wide, small, tiny);
-    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, nbk, boff, active, s), "scan");
-    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, wide, wid, active, s), "scan");
-    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, small, spos, active, s), "scan");
-    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, tiny, tpos, active, s), "scan");
+    scan_arrays({nbk, wide, small, tiny}, {boff, wid, spos, tpos}, active, scan_sums, s);
     k_level_totals<<<1, 1, 0, s>>>(nbk, boff, wide, wid, small, spos, tiny, tpos, active, totals);
     k_small_list<<<blocks_of(active, 256), 256, 0, s>>>(small, spos, tiny, tpos, active, totals, slist);
     check(cudaMemcpyAsync(tot, totals, sizeof(tot), cudaMemcpyDeviceToHost, s), "download");
@@ -1282,15 +1361,14 @@ int SceneBuilder::build_device(const float* d_tris, int n, float* d_bounds, int*
     if (ntiny > 0)
       k_split_tiny<<<blocks_of(ntiny, 2 * kWarpsPerBlock), kBuildBlock, 0, s>>>(
           slist + nsmall, ntiny, slots[cur], order_a, bmin, bmax, cent, d_bounds, d_nodes, split, is_split, bins, live);
-    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, is_split, rank, active, s), "scan");
-    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, live, live_pos, active, s), "scan");
+    scan_arrays({is_split, live}, {rank, live_pos}, active, scan_sums, s);
     check(cudaMemcpyAsync(&pair[0], rank + active - 1, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
     check(cudaMemcpyAsync(&pair[1], is_split + active - 1, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
     check(cudaMemcpyAsync(&lives[0], live_pos + active - 1, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
     check(cudaMemcpyAsync(&lives[1], live + active - 1, sizeof(int), cudaMemcpyDeviceToHost, s), "download");
     if (nwide > 0) {
       k_count_left<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], split, order_a, cent, bins, blk_left);
-      check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, blk_left, blk_pre, nblocks, s), "scan");
+      scan_arrays({blk_left}, {blk_pre}, nblocks, scan_sums, s);
     }
     if (nblocks > 0)
       k_scatter<<<nblocks, kBuildBlock, 0, s>>>(lp, slots[cur], split, rank, total, order_a, order_b, cent, d_nodes,
@@ -1473,7 +1551,7 @@ size_t SceneBuilder::device_bytes() const {
   const BuildBuffers& B = *b_;
   size_t t = B.bmin.n * 16 * 3 + B.order_tmp.n * 4 + (B.slots[0].n + B.slots[1].n) * sizeof(Slot) +
              B.split.n * sizeof(Split) + (B.is_split.n + B.rank.n + B.nb.n + B.boff.n + B.wide.n + B.wid.n) * 4 +
-             (B.blk_left.n + B.blk_pre.n) * 4 + B.acc.n * sizeof(WideAcc) + B.scan_tmp.n + B.p.n * 8 + B.nrm.n * 8 +
+             (B.blk_left.n + B.blk_pre.n) * 4 + B.acc.n * sizeof(WideAcc) + B.scan_sums.n * 4 + B.p.n * 8 + B.nrm.n * 8 +
              B.uv.n * 8 + B.colors.n * 8 + B.tris.n * 4 + B.tris_out.n * 4 + B.nrm_out.n * 4 + B.uv_out.n * 4 +
              B.col_out.n * 4 + B.tan_out.n * 4 + B.bounds.n * 4 + B.nodes.n * 4 + B.mats.n * 4 + B.mats_out.n * 4 +
              B.order.n * 4 + B.flags.n + B.sides.n + B.flags_out.n + B.sides_out.n + B.has_color.n +
