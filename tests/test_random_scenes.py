@@ -15,7 +15,7 @@ tone map and exposure, sRGB or linear output.
 
 GI is off, so each render is deterministic on both sides (same seed, same
 random draws): the RGBA8 images agree within one level on at least 99.9 % of
-pixels (the north_star criterion), and the float samples (tone-mapped,
+pixels (the parity bar for deterministic renders), and the float samples (tone-mapped,
 premultiplied) within 2e-4 on at least 99 %.
 """
 import math

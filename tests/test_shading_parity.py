@@ -3,7 +3,7 @@ texture-sampling answers.
 
 Each case renders one small scene at 1 sample with GI off (deterministic), on
 the oracle and through the C ABI on the GPU, and compares every pixel: the
-RGBA8 bytes within one level (the north_star criterion for deterministic
+RGBA8 bytes within one level (the parity bar for deterministic
 renders), and the Float32 sample sums (tone-mapped, premultiplied RGBA, as
 encodeTile accumulates them, src/progressive.ts:288-313) within a float
 tolerance on at least 99 % of pixels (the GPU computes in FP32, the oracle in
