@@ -7,7 +7,6 @@
 // texture and environment indices are all checked here.
 #include <cuda_runtime.h>
 
-#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <climits>
@@ -1116,13 +1115,8 @@ int32_t mcrt_compile_instances(mcrt_executor* ex, int32_t version, int32_t count
         flag.ensure(sizeof(int) * m_cap);
         index.ensure(sizeof(int) * m_cap);
         k_inner_flags<<<blocks(m, 256), 256, 0, s>>>(g.nodes, m, flag.as<int>());
-        size_t temp_bytes = 0;
-        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, flag.as<int>(), index.as<int>(),
-                                                 static_cast<int>(m_cap), s),
-                   "scan");
-        temp.ensure(temp_bytes);
-        cuda_check(cub::DeviceScan::ExclusiveSum(temp.as<void>(), temp_bytes, flag.as<int>(), index.as<int>(), m, s),
-                   "scan");
+        temp.ensure(sizeof(int) * exclusive_scan_scratch());
+        exclusive_scan(flag.as<int>(), index.as<int>(), m, temp.as<int>(), s);
         G.nodes.ensure(sizeof(DNode) * std::max(n - 1, 1));
         k_pack_nodes<<<blocks(m, 256), 256, 0, s>>>(g.bounds, g.nodes, index.as<int>(), m, G.nodes.as<DNode>());
         cuda_check(cudaGetLastError(), "BVH conversion");

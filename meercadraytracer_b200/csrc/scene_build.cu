@@ -1267,6 +1267,12 @@ void scan_arrays(std::initializer_list<const int*> in, std::initializer_list<int
 
 }  // namespace
 
+void exclusive_scan(const int* in, int* out, int n, int* sums, cudaStream_t s) {
+  scan_arrays({in}, {out}, n, sums, s);
+}
+
+int exclusive_scan_scratch() { return kScanMax * kScanBlocks; }
+
 struct BuildBuffers {
   DevArray<float4> bmin, bmax, cent;
   DevArray<uint32_t> order_tmp;

@@ -85,4 +85,10 @@ class SceneBuilder {
   int last_levels_ = 0;
 };
 
+// Exclusive prefix sums of `in` into `out` (n ints) on stream `s`, with the
+// builder's two-kernel scan; `sums` is scratch of exclusive_scan_scratch()
+// ints.
+void exclusive_scan(const int* in, int* out, int n, int* sums, cudaStream_t s);
+int exclusive_scan_scratch();
+
 }  // namespace mcrt
